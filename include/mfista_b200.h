@@ -1,0 +1,197 @@
+/*
+ * C ABI of the B200 MFISTA solver library (libmfista_b200.so).
+ *
+ * Part 1 replaces the reference's solver entry points one for one: same
+ * names, same argument lists and meanings, same struct RESULT layout, so the
+ * reference's command-line drivers (c/mfista_imaging_{nufft,fft,dft}.c) link
+ * against this library unchanged.  Part 2 adds entry points the reference
+ * does not have (batched solves, a reusable device-resident plan, operator
+ * level calls); they follow the same conventions (caller-owned host arrays,
+ * layouts of the reference) and return a status code.
+ *
+ * All computation runs on the current CUDA device of the calling thread.
+ * There is no CPU fallback: without a usable GPU every entry point fails
+ * (the reference-compatible ones print the error, leave their outputs as
+ * the reference leaves them on error, and set mfista_last_status()).
+ */
+#ifndef MFISTA_B200_H
+#define MFISTA_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* struct RESULT exactly as c/mfista.h:45-66 (field order and types are ABI). */
+struct RESULT {
+  int M;
+  int N;
+  int NX;
+  int NY;
+  int N_active;
+  int maxiter;
+  int ITER;
+  int nonneg;
+  double lambda_l1;
+  double lambda_tv;
+  double lambda_tsv;
+  double sq_error;
+  double mean_sq_error;
+  double l1cost;
+  double tvcost;
+  double tsvcost;
+  double finalcost;
+  double comp_time;
+  double *residual;
+  double Lip_const;
+};
+
+/* ------------------------------------------------------------------------
+ * Part 1: drop-in replacements (FP64, one problem per call).
+ * ------------------------------------------------------------------------ */
+
+/* Replaces mfista_imaging_core_nufft, c/mfista.h:172-178
+ * (implementation c/mfista_nufft_lib.c:909-957). */
+void mfista_imaging_core_nufft(double *u_dx, double *v_dy,
+                               double *vis_r, double *vis_i, double *vis_std,
+                               int M, int NX, int NY, int maxiter, double eps,
+                               double lambda_l1, double lambda_tv, double lambda_tsv,
+                               double cinit, double *xinit, double *xout,
+                               int nonneg_flag, int box_flag, float *cl_box,
+                               struct RESULT *mfista_result);
+
+/* Replaces mfista_imaging_core_fft, c/mfista.h:161-168
+ * (implementation c/mfista_fft_lib.c:701-756).  fftw_plan_flag is accepted
+ * and ignored (there is no FFTW planning on the GPU). */
+void mfista_imaging_core_fft(int *u_idx, int *v_idx,
+                             double *y_r, double *y_i, double *noise_stdev,
+                             int M, int NX, int NY, int maxiter, double eps,
+                             double lambda_l1, double lambda_tv, double lambda_tsv,
+                             double cinit, double *xinit, double *xout,
+                             int nonneg_flag, unsigned int fftw_plan_flag,
+                             int box_flag, float *cl_box,
+                             struct RESULT *mfista_result);
+
+/* Replaces mfista_imaging_core_dft, c/mfista.h:151-157
+ * (implementation c/mfista_dft_lib.c:540-589).  A is column-major M x N.
+ * As in the reference, RESULT.residual is malloc'ed here ([M] doubles) and
+ * owned by the caller; looe_flag is ignored (the reference's LOOE call is
+ * commented out, c/mfista_dft_lib.c:508-531). */
+void mfista_imaging_core_dft(double *y, double *A,
+                             int *M, int *N, int NX, int NY, int maxiter, double eps,
+                             double lambda_l1, double lambda_tv, double lambda_tsv,
+                             double cinit, double *xinit, double *xout,
+                             int nonneg_flag, int looe_flag,
+                             int box_flag, float *cl_box,
+                             struct RESULT *mfista_result);
+
+/* ------------------------------------------------------------------------
+ * Part 2: extensions (no counterpart in the reference unless cited).
+ * ------------------------------------------------------------------------ */
+
+enum mfista_status {
+  MFISTA_OK = 0,
+  MFISTA_ERR_CUDA = 1,       /* a CUDA call failed (no device, launch error ...) */
+  MFISTA_ERR_ARG = 2,        /* invalid argument (sizes, flags, unsupported shape) */
+  MFISTA_ERR_NOMEM = 3,      /* device allocation failed */
+  MFISTA_ERR_BOTH_REG = 4,   /* lambda_tv and lambda_tsv both non-zero */
+  MFISTA_ERR_NONFINITE = 5,  /* objective became NaN/Inf: problem stopped */
+  MFISTA_ERR_STEPCAP = 6     /* device step budget exhausted: problem stopped */
+};
+
+/* Status / message of the last call made by this thread. */
+int mfista_last_status(void);
+const char *mfista_last_error(void);
+
+/* FGP iterations used by the TV form of the drop-in entry points on this
+ * thread (the reference compiles it in: FGPITER 100, c/mfista.h:38).
+ * Returns the previous value; n < 1 is rejected (returns -1). */
+int mfista_set_fgp_iter(int n);
+
+/* Arithmetic of the operators (spread/interp/FFT/stencils).  The objective,
+ * reductions, backtracking test and FISTA sequence are FP64 in both. */
+enum mfista_precision { MFISTA_FP64 = 64, MFISTA_FP32 = 32 };
+
+/* Per-problem parameters of a batched solve. */
+struct mfista_problem {
+  double lambda_l1;
+  double lambda_tv;
+  double lambda_tsv;
+  double cinit;
+  int maxiter;
+  int nonneg_flag;
+  /* > 0: the problem also stops as soon as its accepted objective is
+   * <= target_cost (used to time solves to a given relative objective);
+   * 0 keeps the reference's stopping rules only. */
+  double target_cost;
+};
+
+/* Batched NUFFT solve: B problems on one Nx x Ny grid advance together on
+ * the GPU, each with its own backtracking state and convergence mask.
+ *   geometry: if shared_geometry != 0 all problems use the M points of
+ *     u_dx/v_dy/vis_*; otherwise problem b uses points
+ *     [pt_off[b], pt_off[b+1]) of the concatenated arrays (uneven M).
+ *   eps is scaled per problem exactly as mfista_imaging_core_nufft does.
+ *   xinit: [B*Nx*Ny] or NULL (zero start); xout: [B*Nx*Ny];
+ *   results: [B] RESULT records (residual left NULL).
+ *   fgp_iter: FGP iterations of the TV form (the reference uses 100). */
+int mfista_nufft_batch(const double *u_dx, const double *v_dy, const double *vis_r,
+                       const double *vis_i, const double *vis_std, const int *pt_off,
+                       int shared_geometry, int M, int Nx, int Ny, int B,
+                       const struct mfista_problem *problems, double eps, int precision,
+                       int fgp_iter, const double *xinit, double *xout,
+                       struct RESULT *results);
+
+/* Device-resident plan of a batched NUFFT solve.  Creation uploads the
+ * geometry and visibilities once and builds the CUDA graph; mfista_plan_run
+ * enqueues one whole batched solve on the plan's stream without waiting;
+ * mfista_plan_fetch waits and copies results to the host. */
+typedef struct mfista_plan_s *mfista_plan;
+mfista_plan mfista_nufft_plan_create(const double *u_dx, const double *v_dy,
+                                     const double *vis_r, const double *vis_i,
+                                     const double *vis_std, const int *pt_off,
+                                     int shared_geometry, int M, int Nx, int Ny, int B,
+                                     int precision, int form_tv, int fgp_iter);
+int mfista_plan_set_problems(mfista_plan plan, const struct mfista_problem *problems,
+                             double eps, const double *xinit);
+int mfista_plan_run(mfista_plan plan);
+int mfista_plan_fetch(mfista_plan plan, double *xout, struct RESULT *results);
+void *mfista_plan_stream(mfista_plan plan);          /* cudaStream_t */
+/* Times one operator kernel of the plan in isolation on the plan's stream:
+ * `reps` back-to-back launches over all B problems, CUDA events around
+ * them.  kernel: 0 interpolation, 1 spreading, 2 row FFT (forward),
+ * 3 column FFT (forward), 4 column FFT (inverse), 5 row FFT (inverse),
+ * 6 proximal update (TSV form) or FGP (TV form).  Outputs the mean
+ * milliseconds per launch and the algorithmic bytes one launch must move
+ * (compulsory reads + writes).  Leaves the plan's iterates undefined: call
+ * mfista_plan_set_problems again before the next run. */
+int mfista_plan_profile(mfista_plan plan, int kernel, int reps, double *ms_per_launch,
+                        double *bytes_per_launch);
+int mfista_plan_kernel_launches(mfista_plan plan);   /* kernels per solve, last run */
+void mfista_plan_destroy(mfista_plan plan);
+
+/* Operators of the NUFFT variant, as the C++ reference exports them
+ * (x2y_nufft / y2x_nufft, c++/mfista.hpp:136-140), with the C gridding of
+ * c/mfista_nufft_lib.c:123-243:
+ *   forward: (out_r, out_i)[M] = NUFFT2d2(x)       x: [Nx*Ny]
+ *   adjoint: x_out[Nx*Ny]      = NUFFT2d1(r_r, r_i) */
+int mfista_nufft_forward(const double *u_dx, const double *v_dy, int M, int Nx, int Ny,
+                         const double *x, double *out_r, double *out_i, int precision);
+int mfista_nufft_adjoint(const double *u_dx, const double *v_dy, int M, int Nx, int Ny,
+                         const double *r_r, const double *r_i, double *x_out, int precision);
+
+/* FGP TV proximal map alone (FGP_L1_box / FGP_nonneg_box,
+ * c/mfista_TV_lib.c:189-384) on an NX x NY view: x_out = prox(b). */
+int mfista_fgp_prox(const double *b, int NX, int NY, double lambda_l1, double lambda_tv,
+                    int iters, int nonneg_flag, int box_flag, const float *cl_box,
+                    double *x_out, int precision);
+
+/* Power-iteration estimate of the Lipschitz constant of the chi^2 gradient
+ * (largest eigenvalue of A^H W^2 A) of a NUFFT problem, for choosing cinit. */
+int mfista_nufft_lipschitz(const double *u_dx, const double *v_dy, const double *vis_std,
+                           int M, int Nx, int Ny, int iters, double *lip_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MFISTA_B200_H */

@@ -118,37 +118,54 @@ class NufftPlan:
         return (p[np.ix_(ri, cj)] * self.e4 / self.mm).reshape(-1)
 
     # -- forward: NUFFT2d2 (:187-243) -------------------------------------
+    def _gather_tables(self):
+        """Flat half-grid cells and weights of every (point, ly, lx) tap: the
+        direct cells when the y index lands in the half plane, else the
+        mirrored cell with the opposite sign on the imaginary part."""
+        if getattr(self, "_fwd", None) is None:
+            ny1 = self.ny + 1
+            direct = self.cy_d >= 0
+            col = np.where(direct, self.cy_d, self.cy_m)
+            sgn = np.where(direct, NU_SIGN, -NU_SIGN).astype(np.float64)
+            row = np.where(direct[:, :, None], self.rx_d[:, None, :], self.rx_m[:, None, :])
+            ok = (col[:, :, None] >= 0) & (row >= 0)
+            flat = np.where(ok, row * ny1 + col[:, :, None], 0).reshape(self.m, -1)
+            w = ((self.e1[:, None, None] * self.wy[:, :, None]) * self.wx[:, None, :] / self.mm) * ok
+            self._fwd = (flat, w.reshape(self.m, -1), (w * sgn[:, :, None]).reshape(self.m, -1))
+        return self._fwd
+
     def forward(self, x):
-        g = np.fft.rfft2(self.pad(x))            # FFTW r2c == rfft2 (unnormalised)
-        ny1 = self.ny + 1
-        direct = self.cy_d >= 0                   # per (k, ly)
-        col = np.where(direct, self.cy_d, self.cy_m)            # [M, 24ly]
-        sgn = np.where(direct, NU_SIGN, -NU_SIGN).astype(np.float64)
-        row = np.where(direct[:, :, None], self.rx_d[:, None, :], self.rx_m[:, None, :])
-        ok = (col[:, :, None] >= 0) & (row >= 0)
-        flat = np.where(ok, row * ny1 + col[:, :, None], 0)
-        vals = g.reshape(-1)[flat] * ok
-        w = (self.e1[:, None, None] * self.wy[:, :, None]) * self.wx[:, None, :] / self.mm
-        fr = np.einsum("kyx,kyx->k", w, vals.real)
-        fi = np.einsum("kyx,ky,kyx->k", w, sgn, vals.imag)
-        return fr, fi
+        g = np.fft.rfft2(self.pad(x)).reshape(-1)   # FFTW r2c == rfft2 (unnormalised)
+        flat, wr, wi = self._gather_tables()
+        vals = g[flat]
+        return np.einsum("kt,kt->k", wr, vals.real), np.einsum("kt,kt->k", wi, vals.imag)
 
     # -- adjoint: NUFFT2d1 (:123-185) -------------------------------------
+    def _scatter_tables(self):
+        if getattr(self, "_adj", None) is None:
+            ny1 = self.ny + 1
+            ww = (self.wy[:, :, None] * self.wx[:, None, :]) / 2          # [M, ly, lx]
+            parts = []
+            for rows, cols, conj in ((self.rx_d, self.cy_d, False), (self.rx_m, self.cy_m, True)):
+                ok = (cols[:, :, None] >= 0) & (rows[:, None, :] >= 0)
+                flat = (rows[:, None, :] * ny1 + cols[:, :, None])[ok]
+                kidx = np.broadcast_to(np.arange(self.m)[:, None, None], ok.shape)[ok]
+                parts.append((flat, kidx, ww[ok], conj))
+            self._adj = parts
+        return self._adj
+
     def adjoint(self, fin_r, fin_i):
         nx, ny = self.nx, self.ny
-        ny1 = ny + 1
-        v0 = fin_r * self.e1 + 1j * (NU_SIGN * fin_i * self.e1)
-        vy = v0[:, None] * self.wy                              # [M, 24ly]
-        val = vy[:, :, None] * self.wx[:, None, :] / 2          # [M, ly, lx]
-        size = 2 * nx * ny1
+        size = 2 * nx * (ny + 1)
+        v0 = np.asarray(fin_r) * self.e1 + 1j * (NU_SIGN * np.asarray(fin_i) * self.e1)
         acc = np.zeros(size, np.complex128)
-        for rows, cols, vv in ((self.rx_d, self.cy_d, val), (self.rx_m, self.cy_m, np.conj(val))):
-            ok = (cols[:, :, None] >= 0) & (rows[:, None, :] >= 0)
-            flat = (rows[:, None, :] * ny1 + cols[:, :, None])[ok]
-            vsel = vv[ok]
-            acc += np.bincount(flat, weights=vsel.real, minlength=size)
-            acc += 1j * np.bincount(flat, weights=vsel.imag, minlength=size)
-        g = acc.reshape(2 * nx, ny1)
+        for flat, kidx, w, conj in self._scatter_tables():
+            v = v0[kidx] * w
+            if conj:
+                v = np.conj(v)
+            acc += np.bincount(flat, weights=v.real, minlength=size)
+            acc += 1j * np.bincount(flat, weights=v.imag, minlength=size)
+        g = acc.reshape(2 * nx, ny + 1)
         # FFTW c2r (unnormalised); numpy's irfft2 divides by the size
         p = np.fft.irfft2(g, s=(2 * nx, 2 * ny)) * self.mm
         return self.unpad(p)

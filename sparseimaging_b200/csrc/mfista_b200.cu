@@ -1,0 +1,546 @@
+// C ABI of libmfista_b200.so (declared in include/mfista_b200.h).
+//
+// The three reference entry points keep the reference's argument handling
+// and RESULT bookkeeping (c/mfista_nufft_lib.c:909-957,
+// c/mfista_fft_lib.c:701-756, c/mfista_dft_lib.c:540-589); the iteration
+// itself runs on the GPU through mf::Solver.
+#include <time.h>
+
+#include "solver.cuh"
+
+using namespace mf;
+
+namespace {
+
+thread_local int g_status = 0;
+thread_local std::string g_msg;
+thread_local int g_fgp_iter = 100;  // FGPITER, c/mfista.h:38
+
+void set_ok() {
+  g_status = MFISTA_OK;
+  g_msg.clear();
+}
+
+int fail(int st, const std::string& m, bool print) {
+  g_status = st;
+  g_msg = m;
+  if (print) printf("mfista_b200: %s\n", m.c_str());
+  return st;
+}
+
+bool quiet() {
+  const char* q = getenv("MFISTA_QUIET");
+  return q && q[0] == '1';
+}
+
+double now_s() {
+  timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
+// result summary fields common to the three variants (calc_result_*)
+void fill_result(RESULT* r, const FinalOut& o, int m_report, double m_div, int nx, int ny, int n, double l1,
+                 double ltv, double ltsv, int maxiter, int nonneg, double comp_time, bool skipped, double cinit) {
+  r->M = m_report;
+  r->N = n;
+  r->NX = nx;
+  r->NY = ny;
+  r->lambda_l1 = l1;
+  r->lambda_tv = ltv;
+  r->lambda_tsv = ltsv;
+  r->sq_error = o.sq_error;
+  r->mean_sq_error = o.sq_error / m_div;
+  r->l1cost = o.l1cost;
+  r->N_active = (int)llround(o.n_active);
+  r->finalcost = o.finalcost;
+  if (ltsv > 0) r->tsvcost = o.regcost;
+  else if (ltv > 0) r->tvcost = o.regcost;
+  r->comp_time = comp_time;
+  r->ITER = skipped ? 0 : o.iters;
+  r->nonneg = nonneg;
+  r->Lip_const = skipped ? cinit : o.lip;
+  r->maxiter = maxiter;
+}
+
+template <typename MakeOp>
+void run_single(MakeOp make_op, int N, int NX, int NY, int form, const float* box, const ProbParams& p,
+                const double* x0, bool skip, double* xout, FinalOut& out, double& comp_time) {
+  Solver S;
+  S.precision = MFISTA_FP64;
+  S.init_common(1, N, NX, NY, form, g_fgp_iter, box);
+  S.op.reset(make_op(S.ctx));
+  S.finish_setup();
+  double t0 = now_s();
+  S.upload_problems({p}, x0);
+  S.enqueue_solve(skip);
+  std::vector<FinalOut> o;
+  S.fetch(xout, o);
+  comp_time = now_s() - t0;
+  out = o[0];
+}
+
+}  // namespace
+
+extern "C" int mfista_last_status(void) { return g_status; }
+extern "C" int mfista_set_fgp_iter(int n) {
+  if (n < 1) return -1;
+  int old = g_fgp_iter;
+  g_fgp_iter = n;
+  return old;
+}
+extern "C" const char* mfista_last_error(void) { return g_msg.c_str(); }
+
+// ---------------------------------------------------------------------------
+// drop-in entry points
+// ---------------------------------------------------------------------------
+extern "C" void mfista_imaging_core_nufft(double* u_dx, double* v_dy, double* vis_r, double* vis_i,
+                                          double* vis_std, int M, int Nx, int Ny, int maxiter, double eps,
+                                          double lambda_l1, double lambda_tv, double lambda_tsv, double cinit,
+                                          double* xinit, double* xout, int nonneg_flag, int box_flag,
+                                          float* cl_box, struct RESULT* mfista_result) {
+  set_ok();
+  // epsilon = eps * sum|vis|^2 / M  (:923-926)
+  double sr = 0, si = 0;
+  for (int i = 0; i < M; ++i) sr += vis_r[i] * vis_r[i];
+  for (int i = 0; i < M; ++i) si += vis_i[i] * vis_i[i];
+  double epsilon = sr + si;
+  epsilon *= eps / ((double)M);
+  int form;
+  if (lambda_tv == 0) form = kFormTSV;
+  else if (lambda_tsv == 0) form = kFormTV;
+  else {
+    printf("You cannot set both of lambda_TV and lambda_TSV positive.\n");
+    fail(MFISTA_ERR_BOTH_REG, "lambda_tv and lambda_tsv both non-zero", false);
+    return;
+  }
+  if (maxiter < 0) {
+    fail(MFISTA_ERR_ARG, "maxiter must be >= 0", true);
+    return;
+  }
+  bool skip = form == kFormTSV && nonneg_flag != 0 && nonneg_flag != 1;
+  if (!quiet()) {
+    printf("computing image with MFISTA with NUFFT.\n");
+    printf("stop if iter = %d, or Delta_cost < %e\n", maxiter, epsilon);
+    if (skip) printf("nonneg_flag must be chosen properly.\n");
+  }
+  try {
+    ProbParams p{lambda_l1, lambda_tv, lambda_tsv, cinit, epsilon, maxiter, nonneg_flag, box_flag, 0, 0.0};
+    NufftInput in{u_dx, v_dy, vis_r, vis_i, vis_std, nullptr, 1, M, Nx, Ny};
+    FinalOut o;
+    double ct;
+    std::vector<double> xo(skip ? xout : xinit, (skip ? xout : xinit) + (size_t)Nx * Ny);
+    run_single([&](Ctx& c) { return new NufftOp<double>(c, in); }, Nx * Ny, Nx, Ny, form,
+               box_flag == 1 ? cl_box : nullptr, p, xo.data(), skip, xo.data(), o, ct);
+    memcpy(xout, xo.data(), sizeof(double) * (size_t)Nx * Ny);
+    fill_result(mfista_result, o, M / 2, (double)M, Nx, Ny, Nx * Ny, lambda_l1, lambda_tv, lambda_tsv, maxiter,
+                nonneg_flag, ct, skip, cinit);
+    if (o.status) fail(o.status, "solver stopped early (status " + std::to_string(o.status) + ")", !quiet());
+  } catch (const Error& e) {
+    fail(e.status, e.what(), true);
+  }
+}
+
+extern "C" void mfista_imaging_core_fft(int* u_idx, int* v_idx, double* y_r, double* y_i, double* noise_stdev,
+                                        int M, int NX, int NY, int maxiter, double eps, double lambda_l1,
+                                        double lambda_tv, double lambda_tsv, double cinit, double* xinit,
+                                        double* xout, int nonneg_flag, unsigned int fftw_plan_flag, int box_flag,
+                                        float* cl_box, struct RESULT* mfista_result) {
+  (void)fftw_plan_flag;
+  set_ok();
+  double epsilon = 0;  // (:715-717)
+  for (int i = 0; i < M; ++i) epsilon += y_r[i] * y_r[i] + y_i[i] * y_i[i];
+  epsilon *= eps / ((double)M);
+  int form;
+  if (lambda_tv == 0) form = kFormTSV;
+  else if (lambda_tsv == 0) form = kFormTV;
+  else {
+    printf("You cannot set both of lambda_TV and lambda_TSV positive.\n");
+    fail(MFISTA_ERR_BOTH_REG, "lambda_tv and lambda_tsv both non-zero", false);
+    return;
+  }
+  if (maxiter < 0) {
+    fail(MFISTA_ERR_ARG, "maxiter must be >= 0", true);
+    return;
+  }
+  bool skip = form == kFormTSV && nonneg_flag != 0 && nonneg_flag != 1;
+  if (!quiet()) {
+    printf("computing image with MFISTA.\n");
+    printf("stop if iter = %d, or Delta_cost < %e\n", maxiter, epsilon);
+    if (skip) printf("nonneg_flag must be chosen properly.\n");
+  }
+  try {
+    ProbParams p{lambda_l1, lambda_tv, lambda_tsv, cinit, epsilon, maxiter, nonneg_flag, box_flag, 0, 0.0};
+    FftVarInput in{u_idx, v_idx, y_r, y_i, noise_stdev, M, NX, NY};
+    FinalOut o;
+    double ct;
+    std::vector<double> xo(skip ? xout : xinit, (skip ? xout : xinit) + (size_t)NX * NY);
+    run_single([&](Ctx& c) { return new FftVarOp<double>(c, in); }, NX * NY, NX, NY, form,
+               box_flag == 1 ? cl_box : nullptr, p, xo.data(), skip, xo.data(), o, ct);
+    memcpy(xout, xo.data(), sizeof(double) * (size_t)NX * NY);
+    fill_result(mfista_result, o, M / 2, (double)M, NX, NY, NX * NY, lambda_l1, lambda_tv, lambda_tsv, maxiter,
+                nonneg_flag, ct, skip, cinit);
+    if (o.status) fail(o.status, "solver stopped early (status " + std::to_string(o.status) + ")", !quiet());
+  } catch (const Error& e) {
+    fail(e.status, e.what(), true);
+  }
+}
+
+extern "C" void mfista_imaging_core_dft(double* y, double* A, int* M, int* N, int NX, int NY, int maxiter,
+                                        double eps, double lambda_l1, double lambda_tv, double lambda_tsv,
+                                        double cinit, double* xinit, double* xout, int nonneg_flag, int looe_flag,
+                                        int box_flag, float* cl_box, struct RESULT* mfista_result) {
+  (void)looe_flag;
+  set_ok();
+  int m = *M, n = *N;
+  memcpy(xout, xinit, sizeof(double) * (size_t)n);  // (:552)
+  int form;
+  if (lambda_tv == 0) form = kFormTSV;
+  else if (lambda_tsv == 0) form = kFormTV;
+  else {
+    printf("You cannot set both of lambda_TV and lambda_TSV positive.\n");
+    fail(MFISTA_ERR_BOTH_REG, "lambda_tv and lambda_tsv both non-zero", false);
+    return;
+  }
+  if (maxiter < 0) {
+    fail(MFISTA_ERR_ARG, "maxiter must be >= 0", true);
+    return;
+  }
+  bool skip = form == kFormTSV && nonneg_flag != 0 && nonneg_flag != 1;
+  if (!quiet()) {
+    printf("computing image with MFISTA.\n");
+    if (skip) printf("nonneg_flag must be chosen properly.\n");
+  }
+  try {
+    ProbParams p{lambda_l1, lambda_tv, lambda_tsv, cinit, eps, maxiter, nonneg_flag, box_flag, 0, 0.0};
+    FinalOut o;
+    Solver S;
+    S.precision = MFISTA_FP64;
+    S.init_common(1, n, NX, NY, form, g_fgp_iter, box_flag == 1 ? cl_box : nullptr);
+    DftOp* op = new DftOp(S.ctx, A, y, m, n);
+    S.op.reset(op);
+    S.finish_setup();
+    double t0 = now_s();
+    S.upload_problems({p}, xout);
+    S.enqueue_solve(skip);
+    std::vector<FinalOut> outs;
+    std::vector<double> xo(n);
+    S.fetch(xo.data(), outs);
+    double ct = now_s() - t0;
+    o = outs[0];
+    memcpy(xout, xo.data(), sizeof(double) * (size_t)n);
+    if (!quiet()) printf("summarizing result.\n");
+    fill_result(mfista_result, o, m, (double)m, NX, NY, n, lambda_l1, lambda_tv, lambda_tsv, maxiter, nonneg_flag, ct,
+                skip, cinit);
+    // residual y - A x, owned by the caller (:454)
+    mfista_result->residual = (double*)malloc(sizeof(double) * (size_t)std::max(m, 1));
+    MF_CK(cudaMemcpy(mfista_result->residual, op->g.resid, sizeof(double) * (size_t)m, cudaMemcpyDeviceToHost));
+    if (o.status) fail(o.status, "solver stopped early (status " + std::to_string(o.status) + ")", !quiet());
+  } catch (const Error& e) {
+    fail(e.status, e.what(), true);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// batched plan
+// ---------------------------------------------------------------------------
+struct mfista_plan_s {
+  std::unique_ptr<Solver> S;
+  int B = 0, Nx = 0, Ny = 0;
+  int form = kFormTSV;
+  std::vector<int> m_of;         // points per problem
+  std::vector<double> energy;    // sum |vis|^2 per problem
+  std::vector<ProbParams> prm;
+  double comp_time = 0, t_start = 0;
+  int launches = 0;
+};
+
+extern "C" mfista_plan mfista_nufft_plan_create(const double* u_dx, const double* v_dy, const double* vis_r,
+                                                const double* vis_i, const double* vis_std, const int* pt_off,
+                                                int shared_geometry, int M, int Nx, int Ny, int B, int precision,
+                                                int form_tv, int fgp_iter) {
+  set_ok();
+  try {
+    if (B < 1) throw Error(MFISTA_ERR_ARG, "B must be >= 1");
+    if (precision != MFISTA_FP32 && precision != MFISTA_FP64) throw Error(MFISTA_ERR_ARG, "precision must be 32 or 64");
+    if (!shared_geometry && !pt_off) throw Error(MFISTA_ERR_ARG, "pt_off required without shared geometry");
+    std::unique_ptr<mfista_plan_s> P(new mfista_plan_s);
+    P->B = B;
+    P->Nx = Nx;
+    P->Ny = Ny;
+    P->form = form_tv ? kFormTV : kFormTSV;
+    P->S.reset(new Solver);
+    Solver& S = *P->S;
+    S.precision = precision;
+    S.init_common(B, Nx * Ny, Nx, Ny, P->form, fgp_iter, nullptr);
+    NufftInput in{u_dx, v_dy, vis_r, vis_i, vis_std, pt_off, shared_geometry, M, Nx, Ny};
+    if (precision == MFISTA_FP32) S.op.reset(new NufftOp<float>(S.ctx, in));
+    else S.op.reset(new NufftOp<double>(S.ctx, in));
+    S.finish_setup();
+    P->m_of.resize(B);
+    P->energy.resize(B);
+    for (int b = 0; b < B; ++b) {
+      int lo = shared_geometry ? 0 : pt_off[b];
+      int hi = shared_geometry ? M : pt_off[b + 1];
+      double sr = 0, si = 0;
+      for (int i = lo; i < hi; ++i) sr += vis_r[i] * vis_r[i];
+      for (int i = lo; i < hi; ++i) si += vis_i[i] * vis_i[i];
+      P->m_of[b] = hi - lo;
+      P->energy[b] = sr + si;
+    }
+    return P.release();
+  } catch (const Error& e) {
+    fail(e.status, e.what(), false);
+    return nullptr;
+  }
+}
+
+extern "C" int mfista_plan_set_problems(mfista_plan P, const struct mfista_problem* problems, double eps,
+                                        const double* xinit) {
+  set_ok();
+  if (!P) return fail(MFISTA_ERR_ARG, "null plan", false);
+  try {
+    P->prm.resize(P->B);
+    for (int b = 0; b < P->B; ++b) {
+      const mfista_problem& q = problems[b];
+      if (q.lambda_tv != 0 && q.lambda_tsv != 0) throw Error(MFISTA_ERR_BOTH_REG, "lambda_tv and lambda_tsv both non-zero");
+      if ((P->form == kFormTV) != (q.lambda_tv != 0))
+        throw Error(MFISTA_ERR_ARG, "problem regulariser does not match the plan (TV vs TSV)");
+      if (P->form == kFormTSV && q.nonneg_flag != 0 && q.nonneg_flag != 1)
+        throw Error(MFISTA_ERR_ARG, "nonneg_flag must be 0 or 1");
+      if (q.maxiter < 0) throw Error(MFISTA_ERR_ARG, "maxiter must be >= 0");
+      double epsilon = P->energy[b];
+      epsilon *= eps / ((double)P->m_of[b]);
+      P->prm[b] = ProbParams{q.lambda_l1, q.lambda_tv, q.lambda_tsv, q.cinit, epsilon, q.maxiter, q.nonneg_flag, 0, 0, q.target_cost};
+    }
+    P->S->upload_problems(P->prm, xinit);
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
+extern "C" int mfista_plan_run(mfista_plan P) {
+  set_ok();
+  if (!P) return fail(MFISTA_ERR_ARG, "null plan", false);
+  try {
+    P->t_start = now_s();
+    P->S->steps_host[0] = 0;
+    MF_CK(cudaMemcpyAsync(P->S->d_steps.p, P->S->steps_host, sizeof(P->S->steps_host), cudaMemcpyHostToDevice,
+                          P->S->stream));
+    P->S->enqueue_solve(false);
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
+extern "C" int mfista_plan_fetch(mfista_plan P, double* xout, struct RESULT* results) {
+  set_ok();
+  if (!P) return fail(MFISTA_ERR_ARG, "null plan", false);
+  try {
+    std::vector<FinalOut> o;
+    P->S->fetch(xout, o);
+    P->comp_time = now_s() - P->t_start;
+    long long steps = P->S->steps_taken();
+    P->launches = (int)(P->S->fixed_launches + steps * P->S->per_step_launches);
+    int worst = 0;
+    for (int b = 0; b < P->B; ++b) {
+      const ProbParams& p = P->prm[b];
+      if (results)
+        fill_result(&results[b], o[b], P->m_of[b] / 2, (double)P->m_of[b], P->Nx, P->Ny, P->Nx * P->Ny, p.lambda_l1,
+                    p.lambda_tv, p.lambda_tsv, p.maxiter, p.nonneg, P->comp_time, false, p.cinit);
+      if (results) results[b].residual = nullptr;
+      if (o[b].status) worst = o[b].status;
+    }
+    if (worst) return fail(worst, "a problem stopped early (status " + std::to_string(worst) + ")", false);
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
+extern "C" void* mfista_plan_stream(mfista_plan P) { return P ? (void*)P->S->stream : nullptr; }
+
+extern "C" int mfista_plan_profile(mfista_plan P, int kernel, int reps, double* ms_per_launch,
+                                   double* bytes_per_launch) {
+  set_ok();
+  if (!P) return fail(MFISTA_ERR_ARG, "null plan", false);
+  try {
+    double ms = 0, bytes = 0;
+    P->S->profile_kernel(kernel, std::max(1, reps), ms, bytes);
+    if (ms_per_launch) *ms_per_launch = ms;
+    if (bytes_per_launch) *bytes_per_launch = bytes;
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+extern "C" int mfista_plan_kernel_launches(mfista_plan P) { return P ? P->launches : 0; }
+extern "C" void mfista_plan_destroy(mfista_plan P) { delete P; }
+
+extern "C" int mfista_nufft_batch(const double* u_dx, const double* v_dy, const double* vis_r, const double* vis_i,
+                                  const double* vis_std, const int* pt_off, int shared_geometry, int M, int Nx, int Ny,
+                                  int B, const struct mfista_problem* problems, double eps, int precision,
+                                  int fgp_iter, const double* xinit, double* xout, struct RESULT* results) {
+  int form_tv = B > 0 && problems[0].lambda_tv != 0;
+  mfista_plan P = mfista_nufft_plan_create(u_dx, v_dy, vis_r, vis_i, vis_std, pt_off, shared_geometry, M, Nx, Ny, B,
+                                           precision, form_tv, fgp_iter);
+  if (!P) return g_status;
+  int st = mfista_plan_set_problems(P, problems, eps, xinit);
+  if (st == MFISTA_OK) st = mfista_plan_run(P);
+  if (st == MFISTA_OK) st = mfista_plan_fetch(P, xout, results);
+  int keep = g_status;
+  std::string msg = g_msg;
+  mfista_plan_destroy(P);
+  g_status = keep;
+  g_msg = msg;
+  return st;
+}
+
+// ---------------------------------------------------------------------------
+// operator-level entry points
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+int nufft_apply(const double* u, const double* v, const double* wstd, int M, int Nx, int Ny, const double* x,
+                const double* r_r, const double* r_i, double* out_r, double* out_i, double* x_out) {
+  Solver S;
+  S.precision = sizeof(T) == 4 ? MFISTA_FP32 : MFISTA_FP64;
+  S.init_common(1, Nx * Ny, Nx, Ny, kFormTSV, 100, nullptr);
+  std::vector<double> zero(std::max(M, 1), 0.0), one(std::max(M, 1), 1.0);
+  NufftInput in{u, v, zero.data(), zero.data(), wstd ? wstd : one.data(), nullptr, 1, M, Nx, Ny};
+  NufftOp<T>* op = new NufftOp<T>(S.ctx, in);
+  S.op.reset(op);
+  int slots = std::max({op->chi_slots(), op->tsv_slots(), 1});
+  S.d_part.alloc(sizeof(double) * (size_t)kNumQ * slots);
+  S.ctx.part.p = S.d_part.as<double>();
+  S.ctx.part.slots = slots;
+  S.ctx.part.B = 1;
+  ProbState st;
+  memset(&st, 0, sizeof(st));
+  st.active = 1;
+  st.need_grad = 1;
+  MF_CK(cudaMemcpy(S.ctx.st, &st, sizeof(st), cudaMemcpyHostToDevice));
+  ProbParams p;
+  memset(&p, 0, sizeof(p));
+  MF_CK(cudaMemcpy(S.ctx.prm, &p, sizeof(p), cudaMemcpyHostToDevice));
+  if (x) {
+    MF_CK(cudaMemcpy(S.ctx.x, x, sizeof(double) * (size_t)Nx * Ny, cudaMemcpyHostToDevice));
+    op->forward(S.stream, S.ctx.x, kGateAll, kQChiX, true);
+    std::vector<cplx<T>> y2(std::max(M, 1));
+    MF_CK(cudaMemcpyAsync(y2.data(), op->d_y2.p, sizeof(cplx<T>) * (size_t)M, cudaMemcpyDeviceToHost, S.stream));
+    MF_CK(cudaStreamSynchronize(S.stream));
+    // the residual kernel stored (0 - A x) * w * w with w = 1
+    for (int k = 0; k < M; ++k) {
+      out_r[k] = -(double)y2[k].x;
+      out_i[k] = -(double)y2[k].y;
+    }
+  } else {
+    std::vector<cplx<T>> y2(std::max(M, 1));
+    for (int k = 0; k < M; ++k) y2[k] = mk<T>((T)r_r[k], (T)r_i[k]);
+    MF_CK(cudaMemcpy(op->d_y2.p, y2.data(), sizeof(cplx<T>) * (size_t)M, cudaMemcpyHostToDevice));
+    op->adjoint(S.stream, nullptr, -1);
+    MF_CK(cudaMemcpyAsync(x_out, S.ctx.dfdx, sizeof(double) * (size_t)Nx * Ny, cudaMemcpyDeviceToHost, S.stream));
+    MF_CK(cudaStreamSynchronize(S.stream));
+  }
+  return MFISTA_OK;
+}
+
+}  // namespace
+
+extern "C" int mfista_nufft_forward(const double* u_dx, const double* v_dy, int M, int Nx, int Ny, const double* x,
+                                    double* out_r, double* out_i, int precision) {
+  set_ok();
+  try {
+    if (precision == MFISTA_FP32)
+      return nufft_apply<float>(u_dx, v_dy, nullptr, M, Nx, Ny, x, nullptr, nullptr, out_r, out_i, nullptr);
+    return nufft_apply<double>(u_dx, v_dy, nullptr, M, Nx, Ny, x, nullptr, nullptr, out_r, out_i, nullptr);
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
+extern "C" int mfista_nufft_adjoint(const double* u_dx, const double* v_dy, int M, int Nx, int Ny, const double* r_r,
+                                    const double* r_i, double* x_out, int precision) {
+  set_ok();
+  try {
+    if (precision == MFISTA_FP32)
+      return nufft_apply<float>(u_dx, v_dy, nullptr, M, Nx, Ny, nullptr, r_r, r_i, nullptr, nullptr, x_out);
+    return nufft_apply<double>(u_dx, v_dy, nullptr, M, Nx, Ny, nullptr, r_r, r_i, nullptr, nullptr, x_out);
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
+extern "C" int mfista_nufft_lipschitz(const double* u_dx, const double* v_dy, const double* vis_std, int M, int Nx,
+                                      int Ny, int iters, double* lip_out) {
+  set_ok();
+  try {
+    int n = Nx * Ny;
+    std::vector<double> x(n), g(n), fr(M), fi(M), rr(M), ri(M);
+    uint64_t s = 0x9E3779B97F4A7C15ull;
+    for (int i = 0; i < n; ++i) {
+      s ^= s << 13;
+      s ^= s >> 7;
+      s ^= s << 17;
+      x[i] = (double)(s >> 11) / 9007199254740992.0 - 0.5;
+    }
+    double lam = 0;
+    for (int it = 0; it < iters; ++it) {
+      double nrm = 0;
+      for (double v : x) nrm += v * v;
+      nrm = sqrt(nrm);
+      for (double& v : x) v /= nrm;
+      nufft_apply<double>(u_dx, v_dy, nullptr, M, Nx, Ny, x.data(), nullptr, nullptr, fr.data(), fi.data(), nullptr);
+      for (int k = 0; k < M; ++k) {
+        double w2 = 1.0 / (vis_std[k] * vis_std[k]);
+        rr[k] = fr[k] * w2;
+        ri[k] = fi[k] * w2;
+      }
+      nufft_apply<double>(u_dx, v_dy, nullptr, M, Nx, Ny, nullptr, rr.data(), ri.data(), nullptr, nullptr, g.data());
+      lam = 0;
+      for (int i = 0; i < n; ++i) lam += x[i] * g[i];
+      x = g;
+    }
+    *lip_out = lam;
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
+extern "C" int mfista_fgp_prox(const double* b, int NX, int NY, double lambda_l1, double lambda_tv, int iters,
+                               int nonneg_flag, int box_flag, const float* cl_box, double* x_out, int precision) {
+  set_ok();
+  try {
+    int n = NX * NY;
+    Solver S;
+    S.precision = precision == MFISTA_FP32 ? MFISTA_FP32 : MFISTA_FP64;
+    S.init_common(1, n, NX, NY, kFormTV, iters, box_flag == 1 ? cl_box : nullptr);
+    S.setup_fgp();
+    // FGP forms b = dfdx / c + z (minus lambda_l1 / c when nonneg); with c = 1,
+    // dfdx = 0 and z = b (lambda_l1 = 0 on the nonneg path) it sees b exactly
+    ProbParams p;
+    memset(&p, 0, sizeof(p));
+    p.lambda_l1 = nonneg_flag == 1 ? 0.0 : lambda_l1;
+    p.lambda_tv = lambda_tv;
+    p.nonneg = nonneg_flag;
+    p.box_flag = box_flag;
+    ProbState st;
+    memset(&st, 0, sizeof(st));
+    st.active = 1;
+    st.c = 1.0;
+    MF_CK(cudaMemcpy(S.ctx.prm, &p, sizeof(p), cudaMemcpyHostToDevice));
+    MF_CK(cudaMemcpy(S.ctx.st, &st, sizeof(st), cudaMemcpyHostToDevice));
+    MF_CK(cudaMemcpy(S.ctx.z, b, sizeof(double) * n, cudaMemcpyHostToDevice));
+    MF_CK(cudaMemset(S.ctx.dfdx, 0, sizeof(double) * n));
+    S.launch_fgp(S.stream);
+    MF_CK(cudaMemcpyAsync(x_out, S.ctx.xnew, sizeof(double) * n, cudaMemcpyDeviceToHost, S.stream));
+    MF_CK(cudaStreamSynchronize(S.stream));
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}

@@ -1,0 +1,376 @@
+// Operator-independent MFISTA kernels: the fused gradient-step / proximal /
+// objective-terms kernel of the TSV form, the statistics kernel (|x|_1, TSV or
+// TV, Q-model terms, active pixels), the momentum update, and the FP64
+// control kernel that runs the reference's backtracking, monotone-accept and
+// stopping logic (c/mfista_nufft_lib.c:660-744 and its copies in
+// c/mfista_fft_lib.c and c/mfista_dft_lib.c) for every problem of a batch.
+#pragma once
+#include "common.cuh"
+
+namespace mf {
+
+// soft thresholds (c/mfista_tools.c:81-141), P_positive(_box) in TV_lib
+__device__ __forceinline__ double prox_l1(double v, double eta, int nonneg, const float* box, int f) {
+  if (nonneg == 1) {
+    if (box) return (box[f] == 0.0f || v < eta) ? 0.0 : v - eta;
+    return v < eta ? 0.0 : v - eta;
+  }
+  if (box) {
+    if (box[f] == 0.0f || (v < eta && v > -eta)) return 0.0;
+    return v >= eta ? v - eta : v + eta;
+  }
+  if (v >= eta) return v - eta;
+  if (v <= -eta) return v + eta;
+  return 0.0;
+}
+
+__device__ __forceinline__ double tv_terms_at(const double* __restrict__ x, int f, int NX, int NY) {
+  int i = f % NX, j = f / NX;
+  double xf = x[f];
+  if (i < NX - 1 && j < NY - 1) {
+    double a = xf - x[f + 1], c = xf - x[f + NX];
+    return sqrt(a * a + c * c);
+  }
+  if (j == NY - 1 && i < NX - 1) return fabs(xf - x[f + 1]);
+  if (i == NX - 1 && j < NY - 1) return fabs(xf - x[f + NX]);
+  return 0.0;
+}
+
+__device__ __forceinline__ double tsv_pairs_at(const double* __restrict__ x, int f, int NX, int NY) {
+  int i = f % NX, j = f / NX;
+  double xf = x[f], s = 0.0;
+  if (i < NX - 1) {
+    double d = xf - x[f + 1];
+    s += d * d;
+  }
+  if (j < NY - 1) {
+    double d = xf - x[f + NX];
+    s += d * d;
+  }
+  return s;
+}
+
+// regulariser measured for a problem: 0 none, 1 TSV, 2 TV
+__device__ __forceinline__ int reg_kind(const ProbParams& p, int form, int final_summary) {
+  if (final_summary) {  // calc_result_* (:873-883)
+    if (p.lambda_tsv > 0) return 1;
+    if (p.lambda_tv > 0) return 2;
+    return 0;
+  }
+  if (form == kFormTV) return 2;
+  return p.lambda_tsv > 0 ? 1 : 0;
+}
+
+struct ImgDims {
+  int N;       // pixels
+  int NX, NY;  // TSV/TV view
+  long xstride;
+};
+
+// ---------------------------------------------------------------------------
+// TSV form trial step (c/mfista_nufft_lib.c:684-700):
+//   xtmp = dfdx/c + z ; xnew = soft_th(xtmp, lambda_l1/c)
+// fused with the Q-model dot products (calc_Q_part), |xnew|_1 and TSV(xnew).
+// ---------------------------------------------------------------------------
+__global__ void k_update_tsv(const double* __restrict__ zall, const double* __restrict__ dall,
+                             double* __restrict__ xnall, ImgDims dm, const ProbParams* __restrict__ prm,
+                             const ProbState* __restrict__ st, const float* __restrict__ box, Partials part) {
+  __shared__ double sh[4 * 32];
+  int b = blockIdx.y;
+  if (!gate_ok(st[b], kGateTrial)) return;
+  const ProbParams p = prm[b];
+  const double c = st[b].c;
+  const double cinv = 1.0 / c;
+  const double eta = p.lambda_l1 / c;
+  const double* z = zall + (size_t)b * dm.xstride;
+  const double* d = dall + (size_t)b * dm.xstride;
+  double* xn = xnall + (size_t)b * dm.xstride;
+  const float* bx = p.box_flag == 1 ? box : nullptr;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < dm.N) {
+    double xv = prox_l1(d[f] * cinv + z[f], eta, p.nonneg, bx, f);
+    xn[f] = xv;
+    double df = xv - z[f];
+    v[0] = d[f] * df;
+    v[1] = df * df;
+    v[2] = fabs(xv);
+    if (p.lambda_tsv > 0) {
+      int i = f % dm.NX, j = f / dm.NX;
+      if (i < dm.NX - 1) {
+        double o = prox_l1(d[f + 1] * cinv + z[f + 1], eta, p.nonneg, bx, f + 1);
+        v[3] += (xv - o) * (xv - o);
+      }
+      if (j < dm.NY - 1) {
+        double o = prox_l1(d[f + dm.NX] * cinv + z[f + dm.NX], eta, p.nonneg, bx, f + dm.NX);
+        v[3] += (xv - o) * (xv - o);
+      }
+    }
+  }
+  block_sum<4>(v, sh);
+  if (threadIdx.x == 0) {
+    part.at(kQDq1, b)[blockIdx.x] = v[0];
+    part.at(kQDq2, b)[blockIdx.x] = v[1];
+    part.at(kQL1, b)[blockIdx.x] = v[2];
+    part.at(kQReg, b)[blockIdx.x] = v[3];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// statistics of a vector v: |v|_1, regulariser, active pixels and (optionally)
+// the Q-model dot products against z and dfdx.  Used for the initial cost,
+// the TV form's trial point and the final summary (calc_result_*).
+// ---------------------------------------------------------------------------
+__global__ void k_stats(const double* __restrict__ vall, const double* __restrict__ zall,
+                        const double* __restrict__ dall, ImgDims dm, const ProbParams* __restrict__ prm,
+                        const ProbState* __restrict__ st, int gate, int form, int final_summary, int want_q,
+                        Partials part) {
+  __shared__ double sh[5 * 32];
+  int b = blockIdx.y;
+  if (!gate_ok(st[b], gate)) return;
+  const ProbParams p = prm[b];
+  const double* v = vall + (size_t)b * dm.xstride;
+  int rk = reg_kind(p, form, final_summary);
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < dm.N) {
+    double xv = v[f];
+    acc[2] = fabs(xv);
+    acc[4] = fabs(xv) > 0 ? 1.0 : 0.0;
+    if (rk == 1) acc[3] = tsv_pairs_at(v, f, dm.NX, dm.NY);
+    else if (rk == 2) acc[3] = tv_terms_at(v, f, dm.NX, dm.NY);
+    if (want_q) {
+      const double* z = zall + (size_t)b * dm.xstride;
+      const double* d = dall + (size_t)b * dm.xstride;
+      double df = xv - z[f];
+      acc[0] = d[f] * df;
+      acc[1] = df * df;
+    }
+  }
+  block_sum<5>(acc, sh);
+  if (threadIdx.x == 0) {
+    if (want_q) {
+      part.at(kQDq1, b)[blockIdx.x] = acc[0];
+      part.at(kQDq2, b)[blockIdx.x] = acc[1];
+    }
+    part.at(kQL1, b)[blockIdx.x] = acc[2];
+    part.at(kQReg, b)[blockIdx.x] = acc[3];
+    part.at(kQNact, b)[blockIdx.x] = acc[4];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// momentum (c/mfista_nufft_lib.c:714-739):
+//   monotone improvement: z = x (1-mu)/mu' + xnew (1 + (mu-1)/mu'); x = xnew
+//   otherwise:            z = x (1 - mu/mu') + xnew mu/mu'
+// ---------------------------------------------------------------------------
+__global__ void k_momentum(double* __restrict__ xall, double* __restrict__ zall, const double* __restrict__ xnall,
+                           ImgDims dm, const ProbState* __restrict__ st) {
+  int b = blockIdx.y;
+  const ProbState& s = st[b];
+  if (!s.accepted) return;
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= dm.N) return;
+  double* x = xall + (size_t)b * dm.xstride;
+  double* z = zall + (size_t)b * dm.xstride;
+  const double* xn = xnall + (size_t)b * dm.xstride;
+  double xv = x[f], xnv = xn[f];
+  z[f] = xv * s.mom_a + xnv * s.mom_b;
+  if (s.take_x) x[f] = xnv;
+}
+
+// elementwise copy of a per-problem vector (x = src) for every problem
+__global__ void k_copy_vec(double* __restrict__ dst, const double* __restrict__ src, ImgDims dm) {
+  int b = blockIdx.y;
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < dm.N) dst[(size_t)b * dm.xstride + f] = src[(size_t)b * dm.xstride + f];
+}
+
+// ---------------------------------------------------------------------------
+// control
+// ---------------------------------------------------------------------------
+enum CtrlMode { kCtrlInit = 0, kCtrlStep = 1, kCtrlFinal = 2 };
+
+struct CtrlCfg {
+  int slots[kNumQ];   // partial slots written per quantity
+  double fscale;      // F = fscale * sum(chi partials)
+  int form;
+  int mode;
+  int B;
+  // steps[0]: loop steps taken so far, steps[1]: budget after which every
+  // still-active problem stops (device memory, set per solve)
+  unsigned long long* steps;
+};
+
+// status codes written to ProbState.status (values of enum mfista_status)
+constexpr int kStatusNonFinite = 5;
+constexpr int kStatusStepCap = 6;
+
+struct FinalOut {       // one per problem, read back by the host
+  double sq_error, l1cost, regcost, finalcost;
+  double n_active;
+  double lip;
+  int iters;
+  int status;
+};
+
+__device__ __forceinline__ double warp_partial_sum(const double* p, int n, int lane) {
+  double s = 0.0;
+  for (int i = lane; i < n; i += 32) s += p[i];
+  return warp_sum(s);
+}
+
+__global__ void k_control(const ProbParams* __restrict__ prm, ProbState* __restrict__ st, Partials part,
+                          CtrlCfg cfg, FinalOut* __restrict__ out, cudaGraphConditionalHandle handle,
+                          int set_handle, int* __restrict__ any_active) {
+  __shared__ int s_any, s_cap;
+  if (threadIdx.x == 0) {
+    s_any = 0;
+    s_cap = 0;
+    if (cfg.mode == kCtrlStep && cfg.steps) {
+      unsigned long long n = atomicAdd(cfg.steps, 1ull) + 1ull;
+      if (n >= cfg.steps[1]) s_cap = 1;
+    }
+  }
+  __syncthreads();
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int b = warp; b < cfg.B; b += nw) {
+    ProbState s = st[b];  // every lane reads; lane 0 writes back
+    const ProbParams p = prm[b];
+    if (cfg.mode == kCtrlStep && !s.active) {
+      // finished on an earlier step: its last momentum update already ran
+      if (lane == 0 && s.accepted) st[b].accepted = 0;
+      continue;
+    }
+    double chiX = warp_partial_sum(part.at(kQChiX, b), cfg.slots[kQChiX], lane);
+    double l1 = warp_partial_sum(part.at(kQL1, b), cfg.slots[kQL1], lane);
+    double reg = warp_partial_sum(part.at(kQReg, b), cfg.slots[kQReg], lane);
+    double chiZ = 0, tsvZ = 0, dq1 = 0, dq2 = 0, nact = 0;
+    if (cfg.mode == kCtrlStep) {
+      chiZ = warp_partial_sum(part.at(kQChiZ, b), cfg.slots[kQChiZ], lane);
+      tsvZ = warp_partial_sum(part.at(kQTsvZ, b), cfg.slots[kQTsvZ], lane);
+      dq1 = warp_partial_sum(part.at(kQDq1, b), cfg.slots[kQDq1], lane);
+      dq2 = warp_partial_sum(part.at(kQDq2, b), cfg.slots[kQDq2], lane);
+    }
+    if (cfg.mode == kCtrlFinal) nact = warp_partial_sum(part.at(kQNact, b), cfg.slots[kQNact], lane);
+    if (lane == 0) {
+      const bool tsv_on = cfg.form == kFormTSV && p.lambda_tsv > 0;
+      if (cfg.mode == kCtrlInit) {
+        double cost = cfg.fscale * chiX + p.lambda_l1 * l1;
+        if (cfg.form == kFormTV) cost += p.lambda_tv * reg;
+        else if (tsv_on) cost += p.lambda_tsv * reg;
+        s.cost_now = cost;
+        s.l1x = l1;
+        s.c = p.cinit;
+        s.mu = 1.0;
+        s.iter = 0;
+        s.trial = 0;
+        s.iters_out = 0;
+        s.accepted = 0;
+        s.take_x = 0;
+        s.active = (p.maxiter > 0 && s.status == 0) ? 1 : 0;
+        s.need_grad = s.active;
+      } else if (cfg.mode == kCtrlStep) {
+        if (s.need_grad) {  // a new outer iteration began with this step
+          s.cost[s.iter % kCostRing] = s.cost_now;
+          s.qcore = cfg.fscale * chiZ + (tsv_on ? p.lambda_tsv * tsvZ : 0.0);
+          s.trial = 0;
+          s.need_grad = 0;
+        }
+        s.accepted = 0;
+        double fval = cfg.fscale * chiX + (tsv_on ? p.lambda_tsv * reg : 0.0);
+        double qval = (-dq1 + s.c * dq2 / 2) + s.qcore;
+        if (isnan(fval) || isnan(qval) || s_cap) {
+          // NaN never passes the backtracking test; the reference would retry
+          // maxiter times per iteration.  Stop this problem with a status.
+          s.status = s_cap ? kStatusStepCap : kStatusNonFinite;
+          s.active = 0;
+          s.iters_out = s.iter + 1;
+          st[b] = s;
+          continue;
+        }
+        bool finish = fval <= qval;
+        if (!finish) {
+          s.c *= kEta;
+          s.trial += 1;
+          finish = s.trial >= p.maxiter;  // backtracking loop exhausted
+        }
+        if (finish) {
+          s.c /= kEta;
+          double mu = s.mu;
+          double munew = (1 + sqrt(1 + 4 * mu * mu)) / 2;
+          fval += p.lambda_l1 * l1;
+          if (cfg.form == kFormTV) fval += p.lambda_tv * reg;
+          bool stop = false;
+          if (fval < s.cost[s.iter % kCostRing]) {
+            s.cost_now = fval;
+            s.mom_a = (1 - mu) / munew;
+            s.mom_b = 1 + ((mu - 1) / munew);
+            s.take_x = 1;
+            s.l1x = l1;
+          } else {
+            s.mom_a = 1 - (mu / munew);
+            s.mom_b = mu / munew;
+            s.take_x = 0;
+            if (s.iter > 1 && s.l1x == 0) stop = true;  // "x becomes a 0 vector"
+          }
+          s.accepted = 1;
+          if (!stop && s.iter >= kMinIter &&
+              (s.cost[(s.iter - kTD) % kCostRing] - s.cost[s.iter % kCostRing]) < p.eps)
+            stop = true;
+          if (!stop && p.target > 0 && s.cost_now <= p.target) stop = true;
+          if (stop) {
+            s.active = 0;
+            s.iters_out = s.iter + 1;
+          } else {
+            s.mu = munew;
+            s.iter += 1;
+            if (s.iter >= p.maxiter) {
+              s.active = 0;
+              s.iters_out = p.maxiter;
+            } else {
+              s.need_grad = 1;
+            }
+          }
+        }
+      } else {  // final summary (calc_result_*)
+        FinalOut o;
+        int rk = reg_kind(p, cfg.form, 1);
+        o.sq_error = 2 * (cfg.fscale * chiX);
+        o.l1cost = l1;
+        o.regcost = reg;
+        o.n_active = nact;
+        double fc = o.sq_error / 2;
+        if (p.lambda_l1 > 0) fc += p.lambda_l1 * l1;
+        if (rk == 1) fc += p.lambda_tsv * reg;
+        else if (rk == 2) fc += p.lambda_tv * reg;
+        o.finalcost = fc;
+        o.lip = s.c;
+        o.iters = s.iters_out;
+        o.status = s.status;
+        out[b] = o;
+      }
+      st[b] = s;
+      if (s.active) atomicOr(&s_any, 1);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (set_handle) cudaGraphSetConditional(handle, s_any ? 1u : 0u);
+    if (any_active) *any_active = s_any;
+  }
+}
+
+// initialise a batch's states before the init evaluation
+__global__ void k_init_state(ProbState* st, int B, int bad_nonneg_tsv) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  ProbState s;
+  memset(&s, 0, sizeof(s));
+  s.status = 0;
+  s.active = 0;
+  st[b] = s;
+  (void)bad_nonneg_tsv;
+}
+
+}  // namespace mf

@@ -1,0 +1,426 @@
+// Gaussian-gridding NUFFT kernels (forward A x and adjoint A^H r) of the
+// reference's NUFFT variant (c/mfista_nufft_lib.c:27-304), restructured for
+// the GPU:
+//   * preNUFFT's per-point factors are computed once per solve on the device
+//     and folded into two 24-tap weight vectors per point (wx, wy*E1);
+//   * the centred zero padding and the E4 grid correction are fused into the
+//     first (row) pass of the r2c FFT and the last (row) pass of the c2r FFT,
+//     and both column passes skip the all-zero half of the padded image;
+//   * interpolation (NUFFT2d2) is one warp per uv point, 576 taps over the 32
+//     lanes, complex grid cells read as one 8/16-byte vector;
+//   * spreading (NUFFT2d1) is output-stationary: every CTA owns a tile of
+//     the half-plane grid and gathers the taps of the points binned to it, so
+//     there are no atomics and the result is deterministic.
+#pragma once
+#include "common.cuh"
+#include "fft_smem.cuh"
+
+namespace mf {
+
+// Geometry of a batch of NUFFT problems (points concatenated).
+template <typename T> struct NufftGeom {
+  const int* mx;          // [Mtot]
+  const int* my;          // [Mtot]
+  const T* wx;            // [Mtot*24]  E2x * E3x
+  const T* wy;            // [Mtot*24]  E1 * E2y * E3y
+  const double* vis_r;    // [Mtot]
+  const double* vis_i;    // [Mtot]
+  const double* weight;   // [Mtot]  1 / vis_std
+  const int* pt_lo;       // [B] first point of problem b
+  const int* pt_hi;       // [B] one past its last point
+  const int* tile_ptr;    // CSR over (geometry, tile): [ngeo*ntiles + 1]
+  const int* tile_pts;    // point indices (global) binned to each tile
+  int tile_bstride;       // ntiles, or 0 when all problems share one geometry
+  long y2_bstride;        // per-problem offset of the residual, 0 if not shared
+  const double* e4;       // [Nx*Ny] grid correction (shared by all problems)
+};
+
+// m2mr (c/mfista_nufft_lib.c:42-48)
+__host__ __device__ __forceinline__ int centre_index(int id, int n) { return id < n / 2 ? id + (3 * n) / 2 : id - n / 2; }
+
+// inverse of centre_index over [0, 2n): image index or -1 for padding
+__host__ __device__ __forceinline__ int uncentre_index(int c, int n) {
+  if (c < n - n / 2) return c + n / 2;
+  if (c >= (3 * n) / 2 && c < (3 * n) / 2 + n / 2) return c - (3 * n) / 2;
+  return -1;
+}
+
+// idx_fftw (c/mfista_nufft_lib.c:32-40) for the x axis: m in [-n, n) -> row,
+// anything else is outside the reference's array (dropped: -1).
+__host__ __device__ __forceinline__ int wrap_row(int m, int nx) {
+  if (m >= 0 && m < nx) return m;
+  if (m >= -nx && m < 0) return m + 2 * nx;
+  return -1;
+}
+// y axis as the reference filters it (idx_fftw(m, 2Ny) < Ny+1, :156/:218)
+__host__ __device__ __forceinline__ int half_col(int m, int ny) {
+  if (m >= 0 && m < ny) return m;
+  if (m == -ny) return ny;
+  return -1;
+}
+
+// ---------------------------------------------------------------------------
+// per-point factors (preNUFFT, c/mfista_nufft_lib.c:50-121)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_nufft_prep_points(const double* __restrict__ u, const double* __restrict__ v,
+                                    const int* __restrict__ mx, const int* __restrict__ my, int mtot, int nx,
+                                    int ny, T* __restrict__ wx, T* __restrict__ wy) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= mtot) return;
+  const double pi = 3.14159265358979323846;
+  double mrx = 2.0 * nx, mry = 2.0 * ny;
+  double taux = 12.0 / (double)(nx * nx), tauy = 12.0 / (double)(ny * ny);
+  double e3x_c = (pi / mrx) * (pi / mrx) / taux;
+  double e3y_c = (pi / mry) * (pi / mry) / tauy;
+  double xix = (2 * pi * (double)mx[k]) / mrx;
+  double xiy = (2 * pi * (double)my[k]) / mry;
+  double du = u[k] - xix, dv = v[k] - xiy;
+  double e1 = exp(-(du * du) / (4 * taux) + -(dv * dv) / (4 * tauy));
+  double ax = pi * du / (mrx * taux), ay = pi * dv / (mry * tauy);
+  for (int j = 0; j < kTaps; ++j) {
+    double pw = (double)(j - (kMSP - 1));
+    int l = j - (kMSP - 1);
+    l = l < 0 ? -l : l;
+    double e3x = exp(-e3x_c * (double)(l * l));
+    double e3y = exp(-e3y_c * (double)(l * l));
+    wx[(size_t)k * kTaps + j] = (T)(exp(pw * ax) * e3x);
+    wy[(size_t)k * kTaps + j] = (T)(e1 * exp(pw * ay) * e3y);
+  }
+}
+
+__global__ void k_nufft_prep_e4(double* __restrict__ e4, int nx, int ny) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nx * ny) return;
+  int i = t / ny, j = t - i * ny;
+  const double pi = 3.14159265358979323846;
+  double taux = 12.0 / (double)(nx * nx), tauy = 12.0 / (double)(ny * ny);
+  double coeff = pi / sqrt(taux * tauy);
+  double ti = (double)(i - nx / 2), tj = (double)(j - nx / 2);  // reference uses Nx/2 for both (:78,:82)
+  e4[t] = coeff * exp(taux * ti * ti + tauy * tj * tj);
+}
+
+// ---------------------------------------------------------------------------
+// forward, pass 1: pad + E4 + real FFT of every image row (rows of the
+// 2Nx x 2Ny padded grid that hold image data), written to the half grid.
+//   Row length n1 = 2Ny is transformed as a complex FFT of length h = Ny.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_nufft_rows_fwd(const double* __restrict__ xall, long xstride, const double* __restrict__ e4,
+                                 cplx<T>* __restrict__ gall, long gstride, int nx, int ny, FftDev<T> fh,
+                                 const cplx<T>* __restrict__ tw2h, const ProbState* __restrict__ st, int gate,
+                                 int rows_per_cta) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int b = blockIdx.y;
+  if (!gate_ok(st[b], gate)) return;
+  const int h = ny;
+  const int ld = h + 1;
+  cplx<T>* A = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* Bf = A + (size_t)rows_per_cta * ld;
+  const double* x = xall + (size_t)b * xstride;
+  cplx<T>* g = gall + (size_t)b * gstride;
+  int i0 = blockIdx.x * rows_per_cta;
+  int nrows = min(rows_per_cta, nx - i0);
+  for (int t = threadIdx.x; t < nrows * h; t += blockDim.x) {
+    int rr = t / h, m = t - rr * h;
+    int i = i0 + rr;
+    int j0 = uncentre_index(2 * m, ny), j1 = uncentre_index(2 * m + 1, ny);
+    T a = 0, c = 0;
+    if (j0 >= 0) a = (T)(x[(size_t)i * ny + j0] * e4[(size_t)i * ny + j0]);
+    if (j1 >= 0) c = (T)(x[(size_t)i * ny + j1] * e4[(size_t)i * ny + j1]);
+    A[rr * ld + m] = mk<T>(a, c);
+  }
+  __syncthreads();
+  cplx<T>* Z = smem_fft<T>(A, Bf, fh, ld, nrows, -1);
+  // X[k] = 1/2[(Z_k + conj Z_{h-k}) - i W^k (Z_k - conj Z_{h-k})], W = exp(-2 pi i / 2h)
+  for (int t = threadIdx.x; t < nrows * (h + 1); t += blockDim.x) {
+    int rr = t / (h + 1), k = t - rr * (h + 1);
+    cplx<T> zk = Z[rr * ld + (k == h ? 0 : k)];
+    cplx<T> zc = cconj<T>(Z[rr * ld + (k == 0 ? 0 : h - k)]);
+    cplx<T> e = cadd<T>(zk, zc);
+    cplx<T> o = csub<T>(zk, zc);
+    cplx<T> wo = cmul_si<T>(cmul<T>(tw2h[k], o), -1);
+    cplx<T> X = mk<T>(T(0.5) * (e.x + wo.x), T(0.5) * (e.y + wo.y));
+    int row = centre_index(i0 + rr, nx);
+    g[(size_t)row * (ny + 1) + k] = X;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// column passes: complex FFT of length 2Nx down groups of half-grid columns.
+//   load_pruned: rows of the padded grid that hold no image data are zero and
+//                are not read (forward).
+//   store_pruned: only rows that map back to image rows are written (inverse).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_nufft_cols(cplx<T>* __restrict__ gall, long gstride, int nx, int ny, FftDev<T> f2x, int sign,
+                             int cols_per_cta, int load_pruned, int store_pruned,
+                             const ProbState* __restrict__ st, int gate) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int b = blockIdx.y;
+  if (!gate_ok(st[b], gate)) return;
+  const int n0 = 2 * nx, ncol = ny + 1;
+  const int ld = n0 + 1;
+  cplx<T>* A = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* Bf = A + (size_t)cols_per_cta * ld;
+  cplx<T>* g = gall + (size_t)b * gstride;
+  int c0 = blockIdx.x * cols_per_cta;
+  int nc = min(cols_per_cta, ncol - c0);
+  for (int t = threadIdx.x; t < n0 * cols_per_cta; t += blockDim.x) {
+    int r = t / cols_per_cta, cc = t - r * cols_per_cta;
+    if (cc >= nc) continue;
+    cplx<T> v = mk<T>(0, 0);
+    if (!load_pruned || uncentre_index(r, nx) >= 0) v = g[(size_t)r * ncol + c0 + cc];
+    A[cc * ld + r] = v;
+  }
+  __syncthreads();
+  cplx<T>* R = smem_fft<T>(A, Bf, f2x, ld, nc, sign);
+  for (int t = threadIdx.x; t < n0 * cols_per_cta; t += blockDim.x) {
+    int r = t / cols_per_cta, cc = t - r * cols_per_cta;
+    if (cc >= nc) continue;
+    if (store_pruned && uncentre_index(r, nx) < 0) continue;
+    g[(size_t)r * ncol + c0 + cc] = R[cc * ld + r];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// forward, pass 3: interpolation at the uv points (NUFFT2d2 :212-241) fused
+// with the weighted residual and chi^2 (calc_yAx_nufft / calc_F_part_nufft,
+// :245-285).  In gradient mode the residual weighted once more (dF_dx_nufft
+// :296-299) is stored for the adjoint.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_nufft_interp(NufftGeom<T> geo, const cplx<T>* __restrict__ gall, long gstride, int nx, int ny,
+                               double inv_mm, const ProbState* __restrict__ st, int gate, Partials part, int qchi,
+                               cplx<T>* __restrict__ y2) {
+  __shared__ double sh[32];
+  int b = blockIdx.y;
+  if (!gate_ok(st[b], gate)) return;
+  const cplx<T>* g = gall + (size_t)b * gstride;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  int p0 = geo.pt_lo[b], p1 = geo.pt_hi[b];
+  int k = p0 + blockIdx.x * nwarp + warp;
+  double chi[1] = {0.0};
+  if (k < p1) {
+    int mxk = geo.mx[k], myk = geo.my[k];
+    const T* wxk = geo.wx + (size_t)k * kTaps;
+    const T* wyk = geo.wy + (size_t)k * kTaps;
+    T accr = 0, acci = 0;
+#pragma unroll 6
+    for (int s = 0; s < (kTaps * kTaps) / 32; ++s) {
+      int t = lane + 32 * s;
+      int lx = t / kTaps, ly = t - lx * kTaps;
+      int m = myk + ly - (kMSP - 1);
+      int mxm = mxk + lx - (kMSP - 1);
+      int col = half_col(m, ny), row;
+      T sgn;
+      if (col >= 0) {
+        row = wrap_row(mxm, nx);
+        sgn = T(-1);  // NU_SIGN
+      } else {
+        col = half_col(-m, ny);
+        row = wrap_row(-mxm, nx);
+        sgn = T(1);
+      }
+      if (col >= 0 && row >= 0) {
+        cplx<T> gv = g[(size_t)row * (ny + 1) + col];
+        T w = wyk[ly] * wxk[lx];
+        accr += gv.x * w;
+        acci += sgn * gv.y * w;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      accr += __shfl_xor_sync(0xffffffffu, accr, o);
+      acci += __shfl_xor_sync(0xffffffffu, acci, o);
+    }
+    if (lane == 0) {
+      double fr = (double)accr * inv_mm, fi = (double)acci * inv_mm;
+      double w = geo.weight[k];
+      double rr = (geo.vis_r[k] - fr) * w;
+      double ri = (geo.vis_i[k] - fi) * w;
+      chi[0] = rr * rr + ri * ri;
+      if (y2) y2[b * geo.y2_bstride + k] = mk<T>((T)(rr * w), (T)(ri * w));
+    }
+  }
+  block_sum<1>(chi, sh);
+  if (threadIdx.x == 0) part.at(qchi, b)[blockIdx.x] = chi[0];
+}
+
+// ---------------------------------------------------------------------------
+// adjoint, pass 1: spreading (NUFFT2d1 :140-171), output-stationary.
+// One thread per half-grid cell of a TR x TC tile; points of the tile's bin
+// are staged through shared memory in chunks.
+// ---------------------------------------------------------------------------
+template <typename T> struct SpreadChunk {
+  static constexpr int P = sizeof(T) == 8 ? 32 : 64;
+};
+
+template <typename T>
+__global__ void k_nufft_spread(NufftGeom<T> geo, const cplx<T>* __restrict__ y2, cplx<T>* __restrict__ gall,
+                               long gstride, int nx, int ny, int tile_r, int tile_c, int ntiles,
+                               const ProbState* __restrict__ st, int gate) {
+  constexpr int P = SpreadChunk<T>::P;
+  __shared__ int s_mx[P], s_my[P];
+  __shared__ T s_vr[P], s_vi[P];
+  __shared__ T s_wx[P][kTaps], s_wy[P][kTaps];
+  int b = blockIdx.y;
+  if (!gate_ok(st[b], gate)) return;
+  cplx<T>* g = gall + (size_t)b * gstride;
+  int tile = blockIdx.x;
+  int ntc = (ny + 1 + tile_c - 1) / tile_c;
+  int tr = tile / ntc, tc = tile - tr * ntc;
+  int ty = threadIdx.x / tile_c, tx = threadIdx.x - ty * tile_c;
+  int row = tr * tile_r + ty, col = tc * tile_c + tx;
+  bool valid = ty < tile_r && row < 2 * nx && col <= ny;
+  int mrow = row < nx ? row : row - 2 * nx;  // x index m with wrap_row(m) == row
+  int mcol = col < ny ? col : -ny;          // y index m with half_col(m) == col
+  T ar = 0, ai = 0;
+  int beg = geo.tile_ptr[(size_t)b * geo.tile_bstride + tile];
+  int end = geo.tile_ptr[(size_t)b * geo.tile_bstride + tile + 1];
+  const cplx<T>* yb = y2 + b * geo.y2_bstride;
+  for (int c0 = beg; c0 < end; c0 += P) {
+    int np = min(P, end - c0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < np; t += blockDim.x) {
+      int k = geo.tile_pts[c0 + t];
+      s_mx[t] = geo.mx[k];
+      s_my[t] = geo.my[k];
+      cplx<T> r = yb[k];
+      s_vr[t] = r.x;
+      s_vi[t] = -r.y;  // NU_SIGN * Fin_i
+    }
+    for (int t = threadIdx.x; t < np * kTaps; t += blockDim.x) {
+      int pp = t / kTaps, j = t - pp * kTaps;
+      int k = geo.tile_pts[c0 + pp];
+      s_wx[pp][j] = geo.wx[(size_t)k * kTaps + j];
+      s_wy[pp][j] = geo.wy[(size_t)k * kTaps + j];
+    }
+    __syncthreads();
+    if (valid) {
+      for (int pp = 0; pp < np; ++pp) {
+        int mx = s_mx[pp], my = s_my[pp];
+        int lxd = mrow - mx + (kMSP - 1), lyd = mcol - my + (kMSP - 1);
+        int lxm = -mrow - mx + (kMSP - 1), lym = -mcol - my + (kMSP - 1);
+        bool d = (unsigned)lxd < (unsigned)kTaps && (unsigned)lyd < (unsigned)kTaps;
+        bool mi = (unsigned)lxm < (unsigned)kTaps && (unsigned)lym < (unsigned)kTaps;
+        if (!(d || mi)) continue;
+        T vr = s_vr[pp], vi = s_vi[pp];
+        // the reference adds the two contributions of one point in ly order
+        // (direct first on a tie), which is kept here
+        if (d && (!mi || lyd <= lym)) {
+          T wy = s_wy[pp][lyd], wx = s_wx[pp][lxd];
+          ar += (vr * wy) * wx * T(0.5);
+          ai += (vi * wy) * wx * T(0.5);
+          d = false;
+        }
+        if (mi) {
+          T wy = s_wy[pp][lym], wx = s_wx[pp][lxm];
+          ar += (vr * wy) * wx * T(0.5);
+          ai -= (vi * wy) * wx * T(0.5);
+        }
+        if (d) {
+          T wy = s_wy[pp][lyd], wx = s_wx[pp][lxd];
+          ar += (vr * wy) * wx * T(0.5);
+          ai += (vi * wy) * wx * T(0.5);
+        }
+      }
+    }
+  }
+  if (valid) g[(size_t)row * (ny + 1) + col] = mk<T>(ar, ai);
+}
+
+// ---------------------------------------------------------------------------
+// adjoint, last pass: half-complex -> real FFT of the rows that map to image
+// rows, unpad, E4/MM (:175-183), and — for the TSV form — the TSV gradient of
+// z folded in (dfdx -= lambda_tsv * d_TSV(z), c/mfista_nufft_lib.c:674-681)
+// together with TSV(z).
+// ---------------------------------------------------------------------------
+struct TsvFuse {
+  const double* z;     // per-problem z (stride xstride) or null
+  const ProbParams* prm;
+  int NX, NY;          // TSV view (reference's TSV(NX, NY, x))
+};
+
+__device__ __forceinline__ double dtsv_at(const double* __restrict__ x, int f, int NX, int NY) {
+  int i = f % NX, j = f / NX;
+  double xf = x[f];
+  double d = (i < NX - 1) ? 2 * (xf - x[f + 1]) : 0.0;
+  if (i >= 1) d += 2 * (xf - x[f - 1]);
+  if (j < NY - 1) d += 2 * (xf - x[f + NX]);
+  if (j >= 1) d += 2 * (xf - x[f - NX]);
+  return d;
+}
+
+__device__ __forceinline__ double tsv_terms_at(const double* __restrict__ x, int f, int NX, int NY) {
+  int i = f % NX, j = f / NX;
+  double xf = x[f], s = 0.0;
+  if (i < NX - 1) {
+    double d = xf - x[f + 1];
+    s += d * d;
+  }
+  if (j < NY - 1) {
+    double d = xf - x[f + NX];
+    s += d * d;
+  }
+  return s;
+}
+
+template <typename T>
+__global__ void k_nufft_rows_inv(const cplx<T>* __restrict__ gall, long gstride, double* __restrict__ dall,
+                                 long xstride, const double* __restrict__ e4, int nx, int ny, double inv_mm,
+                                 FftDev<T> fh, const cplx<T>* __restrict__ tw2h, TsvFuse tf, Partials part,
+                                 int qtsv, const ProbState* __restrict__ st, int gate, int rows_per_cta) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double sh[32];
+  int b = blockIdx.y;
+  if (!gate_ok(st[b], gate)) return;
+  const int h = ny, ld = h + 1;
+  cplx<T>* A = reinterpret_cast<cplx<T>*>(smem_raw);
+  cplx<T>* Bf = A + (size_t)rows_per_cta * ld;
+  const cplx<T>* g = gall + (size_t)b * gstride;
+  double* dfdx = dall + (size_t)b * xstride;
+  int i0 = blockIdx.x * rows_per_cta;
+  int nrows = min(rows_per_cta, nx - i0);
+  // Z[k] = (X_k + conj X_{h-k}) + i conj(W^k) (X_k - conj X_{h-k}); DC/Nyquist real parts only
+  for (int t = threadIdx.x; t < nrows * h; t += blockDim.x) {
+    int rr = t / h, k = t - rr * h;
+    const cplx<T>* grow = g + (size_t)centre_index(i0 + rr, nx) * (ny + 1);
+    cplx<T> xk = grow[k];
+    cplx<T> xc = grow[h - k];
+    if (k == 0) {
+      xk.y = 0;
+      xc.y = 0;
+    }
+    xc = cconj<T>(xc);
+    cplx<T> e = cadd<T>(xk, xc);
+    cplx<T> o = cmul_si<T>(cmul<T>(cconj<T>(tw2h[k]), csub<T>(xk, xc)), 1);
+    A[rr * ld + k] = cadd<T>(e, o);
+  }
+  __syncthreads();
+  cplx<T>* Z = smem_fft<T>(A, Bf, fh, ld, nrows, +1);
+  const ProbParams& pp = tf.prm[b];
+  bool fuse = tf.z != nullptr && pp.lambda_tsv > 0.0;
+  const double* z = fuse ? tf.z + (size_t)b * xstride : nullptr;
+  double acc[1] = {0.0};
+  for (int t = threadIdx.x; t < nrows * ny; t += blockDim.x) {
+    int rr = t / ny, j = t - rr * ny;
+    int i = i0 + rr;
+    int c = centre_index(j, ny);
+    cplx<T> zc = Z[rr * ld + (c >> 1)];
+    double val = (double)((c & 1) ? zc.y : zc.x);
+    int f = i * ny + j;
+    double d = val * e4[f] * inv_mm;
+    if (fuse) {
+      d = d + dtsv_at(z, f, tf.NX, tf.NY) * (-pp.lambda_tsv);
+      acc[0] += tsv_terms_at(z, f, tf.NX, tf.NY);
+    }
+    dfdx[f] = d;
+  }
+  if (qtsv >= 0) {
+    block_sum<1>(acc, sh);
+    if (threadIdx.x == 0) part.at(qtsv, b)[blockIdx.x] = acc[0];
+  }
+}
+
+}  // namespace mf

@@ -1,0 +1,896 @@
+// Host side of the solver: FFT plans, the three operators (NUFFT, gridded
+// FFT, dense DFT), and the batched MFISTA driver that records one MFISTA
+// step as a CUDA graph body and repeats it on the device with a conditional
+// WHILE node until every problem of the batch has stopped.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "dft_ops.cuh"
+#include "fft_smem.cuh"
+#include "fftvar_ops.cuh"
+#include "fgp.cuh"
+#include "mfista_ops.cuh"
+#include "nufft_ops.cuh"
+
+#include "../../include/mfista_b200.h"
+
+namespace mf {
+
+struct Error : std::runtime_error {
+  int status;
+  Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+#define MF_CK(x)                                                                                          \
+  do {                                                                                                    \
+    cudaError_t e_ = (x);                                                                                 \
+    if (e_ != cudaSuccess)                                                                                \
+      throw ::mf::Error(e_ == cudaErrorMemoryAllocation ? MFISTA_ERR_NOMEM : MFISTA_ERR_CUDA,             \
+                        std::string(#x) + ": " + cudaGetErrorString(e_));                                 \
+  } while (0)
+
+#define MF_LAUNCH_CK() MF_CK(cudaGetLastError())
+
+struct DevMem {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevMem() {}
+  DevMem(const DevMem&) = delete;
+  DevMem& operator=(const DevMem&) = delete;
+  ~DevMem() { release(); }
+  void alloc(size_t n) {
+    release();
+    if (n) MF_CK(cudaMalloc(&p, n));
+    bytes = n;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <typename U> U* as() const { return reinterpret_cast<U*>(p); }
+  template <typename U> void upload(const U* h, size_t count) {
+    alloc(count * sizeof(U));
+    if (count) MF_CK(cudaMemcpy(p, h, count * sizeof(U), cudaMemcpyHostToDevice));
+  }
+};
+
+inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------
+// FFT plans
+// ---------------------------------------------------------------------------
+template <typename T> void make_twiddles(int n, DevMem& mem) {
+  std::vector<cplx<T>> h(std::max(n, 1));
+  for (int k = 0; k < n; ++k) {
+    long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
+    h[k] = mk<T>((T)cosl(a), (T)(-sinl(a)));
+  }
+  mem.upload(h.data(), h.size());
+}
+
+template <typename T> struct FftHost {
+  FftDev<T> dev;
+  DevMem tw;
+  void init(int n) {
+    memset(&dev, 0, sizeof(dev));
+    dev.n = n;
+    int m = n;
+    auto push = [&](int r) {
+      if (dev.nst >= kMaxStages) throw Error(MFISTA_ERR_ARG, "FFT length has too many factors");
+      dev.radix[dev.nst++] = r;
+    };
+    while (m % 4 == 0) { push(4); m /= 4; }
+    while (m % 2 == 0) { push(2); m /= 2; }
+    while (m % 3 == 0) { push(3); m /= 3; }
+    while (m % 5 == 0) { push(5); m /= 5; }
+    for (int f = 7; m > 1 && f <= kMaxGenericRadix; f += 2)
+      while (m % f == 0) { push(f); m /= f; }
+    if (m > 1) throw Error(MFISTA_ERR_ARG, "FFT length " + std::to_string(n) + " has a prime factor above 16");
+    make_twiddles<T>(n, tw);
+    dev.tw = tw.as<cplx<T>>();
+  }
+};
+
+template <typename K> void set_smem(K kernel, size_t bytes) {
+  if (bytes > 227 * 1024) throw Error(MFISTA_ERR_ARG, "grid too large for the shared-memory FFT");
+  MF_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+// ---------------------------------------------------------------------------
+// common solver context shared by the operators
+// ---------------------------------------------------------------------------
+struct Ctx {
+  int B = 0;
+  int N = 0;
+  long xstride = 0;
+  int tsvNX = 0, tsvNY = 0;  // TSV/TV view (reference's NX, NY)
+  double* x = nullptr;
+  double* z = nullptr;
+  double* xnew = nullptr;
+  double* dfdx = nullptr;
+  ProbParams* prm = nullptr;
+  ProbState* st = nullptr;
+  Partials part{};
+};
+
+struct Op {
+  virtual ~Op() {}
+  // chi^2 partials of `src` into part[qchi]; `store` keeps the weighted
+  // residual for the next adjoint()
+  virtual void forward(cudaStream_t s, const double* src, int gate, int qchi, bool store) = 0;
+  // gradient at z into ctx.dfdx (gate: need_grad); TSV fused when z_tsv != 0
+  virtual void adjoint(cudaStream_t s, const double* z_tsv, int qtsv) = 0;
+  virtual int chi_slots() const = 0;
+  virtual int tsv_slots() const = 0;
+  virtual double fscale() const = 0;
+  virtual int launches_forward() const = 0;
+  virtual int launches_adjoint() const = 0;
+  // one kernel alone (profiling): 0 interp, 1 spread, 2 rows fwd, 3 cols fwd,
+  // 4 cols inv, 5 rows inv; returns its algorithmic bytes (compulsory reads
+  // and writes of one launch over the whole batch), or < 0 if not defined
+  virtual double launch_single(cudaStream_t s, int kernel) { (void)s; (void)kernel; return -1; }
+};
+
+// ---------------------------------------------------------------------------
+// NUFFT operator
+// ---------------------------------------------------------------------------
+struct NufftInput {
+  const double *u, *v, *vis_r, *vis_i, *vis_std;
+  const int* pt_off;  // B+1 (independent geometry) or null
+  int shared;
+  int M;              // points per problem (shared) or total
+  int Nx, Ny;
+};
+
+// host binning of points to spread tiles (direct and mirrored footprints)
+inline void bin_points(const std::vector<int>& mx, const std::vector<int>& my, int lo, int hi, int nx, int ny,
+                       int tile_r, int tile_c, std::vector<std::vector<int>>& lists) {
+  int ntc = cdiv(ny + 1, tile_c);
+  std::vector<int> tr, tc, ids;
+  for (int k = lo; k < hi; ++k) {
+    ids.clear();
+    for (int mir = 0; mir < 2; ++mir) {
+      tr.clear();
+      tc.clear();
+      int sg = mir ? -1 : 1;
+      for (int l = 0; l < kTaps; ++l) {
+        int r = wrap_row(sg * (mx[k] + l - (kMSP - 1)), nx);
+        if (r >= 0) tr.push_back(r / tile_r);
+        int c = half_col(sg * (my[k] + l - (kMSP - 1)), ny);
+        if (c >= 0) tc.push_back(c / tile_c);
+      }
+      std::sort(tr.begin(), tr.end());
+      tr.erase(std::unique(tr.begin(), tr.end()), tr.end());
+      std::sort(tc.begin(), tc.end());
+      tc.erase(std::unique(tc.begin(), tc.end()), tc.end());
+      for (int a : tr)
+        for (int c : tc) ids.push_back(a * ntc + c);
+    }
+    std::sort(ids.begin(), ids.end());
+    ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+    for (int t : ids) lists[t].push_back(k);
+  }
+}
+
+template <typename T> struct NufftOp : Op {
+  Ctx& c;
+  int nx, ny, B, mtot, mmax;
+  bool shared;
+  DevMem d_u, d_v, d_mx, d_my, d_wx, d_wy, d_vr, d_vi, d_w, d_lo, d_hi, d_tptr, d_tpts, d_e4, d_grid, d_y2, tw2h;
+  FftHost<T> fh, fcol;
+  NufftGeom<T> geo{};
+  int rpc = 8, cpc = 8, tile_r = 8, tile_c = 32, ntiles = 0;
+  size_t smem_rows = 0, smem_cols = 0;
+  long gstride = 0;
+  double inv_mm = 0;
+
+  NufftOp(Ctx& ctx, const NufftInput& in) : c(ctx) {
+    nx = in.Nx;
+    ny = in.Ny;
+    B = ctx.B;
+    shared = in.shared != 0;
+    if (nx < 12 || ny < 12) throw Error(MFISTA_ERR_ARG, "NUFFT needs Nx, Ny >= 12");
+    mtot = in.M;
+    std::vector<int> lo(B), hi(B);
+    if (shared) {
+      for (int b = 0; b < B; ++b) { lo[b] = 0; hi[b] = mtot; }
+    } else {
+      mtot = in.pt_off[B];
+      for (int b = 0; b < B; ++b) { lo[b] = in.pt_off[b]; hi[b] = in.pt_off[b + 1]; }
+    }
+    mmax = 0;
+    for (int b = 0; b < B; ++b) mmax = std::max(mmax, hi[b] - lo[b]);
+    // grid indices of the points (preNUFFT :92-96), on the host so that the
+    // binning below and the device agree exactly
+    std::vector<int> mx(mtot), my(mtot);
+    const double pi = 3.14159265358979323846;
+    double mrx = 2.0 * nx, mry = 2.0 * ny;
+    for (int k = 0; k < mtot; ++k) {
+      mx[k] = (int)round(in.u[k] * mrx / (2 * pi));
+      my[k] = (int)round(in.v[k] * mry / (2 * pi));
+    }
+    std::vector<double> w(mtot);
+    for (int k = 0; k < mtot; ++k) w[k] = 1 / in.vis_std[k];
+    d_u.upload(in.u, mtot);
+    d_v.upload(in.v, mtot);
+    d_mx.upload(mx.data(), mtot);
+    d_my.upload(my.data(), mtot);
+    d_vr.upload(in.vis_r, mtot);
+    d_vi.upload(in.vis_i, mtot);
+    d_w.upload(w.data(), mtot);
+    d_lo.upload(lo.data(), B);
+    d_hi.upload(hi.data(), B);
+    d_wx.alloc(sizeof(T) * (size_t)std::max(mtot, 1) * kTaps);
+    d_wy.alloc(sizeof(T) * (size_t)std::max(mtot, 1) * kTaps);
+    if (mtot > 0) {
+      k_nufft_prep_points<T><<<cdiv(mtot, 256), 256>>>(d_u.as<double>(), d_v.as<double>(), d_mx.as<int>(),
+                                                        d_my.as<int>(), mtot, nx, ny, d_wx.as<T>(), d_wy.as<T>());
+      MF_LAUNCH_CK();
+    }
+    d_e4.alloc(sizeof(double) * nx * ny);
+    k_nufft_prep_e4<<<cdiv(nx * ny, 256), 256>>>(d_e4.as<double>(), nx, ny);
+    MF_LAUNCH_CK();
+    // spread tiles
+    ntiles = cdiv(2 * nx, tile_r) * cdiv(ny + 1, tile_c);
+    int ngeo = shared ? 1 : B;
+    std::vector<int> tptr;
+    std::vector<int> tpts;
+    tptr.reserve((size_t)ngeo * ntiles + 1);
+    tptr.push_back(0);
+    for (int g = 0; g < ngeo; ++g) {
+      std::vector<std::vector<int>> lists(ntiles);
+      bin_points(mx, my, lo[g], hi[g], nx, ny, tile_r, tile_c, lists);
+      for (int t = 0; t < ntiles; ++t) {
+        tpts.insert(tpts.end(), lists[t].begin(), lists[t].end());
+        tptr.push_back((int)tpts.size());
+      }
+    }
+    d_tptr.upload(tptr.data(), tptr.size());
+    d_tpts.upload(tpts.data(), std::max<size_t>(tpts.size(), 1));
+    // FFTs: rows as complex length Ny, columns length 2Nx
+    fh.init(ny);
+    fcol.init(2 * nx);
+    make_twiddles<T>(2 * ny, tw2h);
+    gstride = (long)2 * nx * (ny + 1);
+    d_grid.alloc(sizeof(cplx<T>) * (size_t)B * gstride);
+    long y2n = shared ? (long)B * std::max(mtot, 1) : std::max(mtot, 1);
+    d_y2.alloc(sizeof(cplx<T>) * (size_t)y2n);
+    inv_mm = 1.0 / ((double)(2 * nx) * (double)(2 * ny));
+    // launch shapes: keep the ping-pong buffers within shared memory
+    auto rows_smem = [&](int r) { return (size_t)2 * r * (ny + 1) * sizeof(cplx<T>); };
+    auto cols_smem = [&](int cc) { return (size_t)2 * cc * (2 * nx + 1) * sizeof(cplx<T>); };
+    while (rpc > 1 && rows_smem(rpc) > 96 * 1024) rpc /= 2;
+    while (cpc > 1 && cols_smem(cpc) > 96 * 1024) cpc /= 2;
+    smem_rows = rows_smem(rpc);
+    smem_cols = cols_smem(cpc);
+    set_smem(k_nufft_rows_fwd<T>, smem_rows);
+    set_smem(k_nufft_rows_inv<T>, smem_rows);
+    set_smem(k_nufft_cols<T>, smem_cols);
+    geo.mx = d_mx.as<int>();
+    geo.my = d_my.as<int>();
+    geo.wx = d_wx.as<T>();
+    geo.wy = d_wy.as<T>();
+    geo.vis_r = d_vr.as<double>();
+    geo.vis_i = d_vi.as<double>();
+    geo.weight = d_w.as<double>();
+    geo.pt_lo = d_lo.as<int>();
+    geo.pt_hi = d_hi.as<int>();
+    geo.tile_ptr = d_tptr.as<int>();
+    geo.tile_pts = d_tpts.as<int>();
+    geo.tile_bstride = shared ? 0 : ntiles;
+    geo.y2_bstride = shared ? mtot : 0;
+    geo.e4 = d_e4.as<double>();
+    MF_CK(cudaDeviceSynchronize());
+  }
+
+  int interp_blocks() const { return std::max(1, cdiv(mmax, 8)); }
+
+  void forward(cudaStream_t s, const double* src, int gate, int qchi, bool store) override {
+    cplx<T>* g = d_grid.as<cplx<T>>();
+    k_nufft_rows_fwd<T><<<dim3(cdiv(nx, rpc), B), 256, smem_rows, s>>>(src, c.xstride, geo.e4, g, gstride, nx, ny,
+                                                                       fh.dev, tw2h.as<cplx<T>>(), c.st, gate, rpc);
+    MF_LAUNCH_CK();
+    k_nufft_cols<T><<<dim3(cdiv(ny + 1, cpc), B), 256, smem_cols, s>>>(g, gstride, nx, ny, fcol.dev, -1, cpc, 1, 0,
+                                                                       c.st, gate);
+    MF_LAUNCH_CK();
+    k_nufft_interp<T><<<dim3(interp_blocks(), B), 256, 0, s>>>(geo, g, gstride, nx, ny, inv_mm, c.st, gate, c.part,
+                                                               qchi, store ? d_y2.as<cplx<T>>() : nullptr);
+    MF_LAUNCH_CK();
+  }
+
+  void adjoint(cudaStream_t s, const double* z_tsv, int qtsv) override {
+    cplx<T>* g = d_grid.as<cplx<T>>();
+    k_nufft_spread<T><<<dim3(ntiles, B), tile_r * tile_c, 0, s>>>(geo, d_y2.as<cplx<T>>(), g, gstride, nx, ny,
+                                                                  tile_r, tile_c, ntiles, c.st, kGateGrad);
+    MF_LAUNCH_CK();
+    k_nufft_cols<T><<<dim3(cdiv(ny + 1, cpc), B), 256, smem_cols, s>>>(g, gstride, nx, ny, fcol.dev, +1, cpc, 0, 1,
+                                                                       c.st, kGateGrad);
+    MF_LAUNCH_CK();
+    TsvFuse tf{z_tsv, c.prm, c.tsvNX, c.tsvNY};
+    k_nufft_rows_inv<T><<<dim3(cdiv(nx, rpc), B), 256, smem_rows, s>>>(
+        g, gstride, c.dfdx, c.xstride, geo.e4, nx, ny, inv_mm, fh.dev, tw2h.as<cplx<T>>(), tf, c.part, qtsv, c.st,
+        kGateGrad, rpc);
+    MF_LAUNCH_CK();
+  }
+
+  int chi_slots() const override { return interp_blocks(); }
+  int tsv_slots() const override { return cdiv(nx, rpc); }
+  double fscale() const override { return 0.5; }
+  int launches_forward() const override { return 3; }
+  int launches_adjoint() const override { return 3; }
+
+  double launch_single(cudaStream_t s, int kernel) override {
+    cplx<T>* g = d_grid.as<cplx<T>>();
+    const double cs = sizeof(cplx<T>), ts = sizeof(T);
+    const double G = (double)gstride, N = (double)nx * ny, half_rows = (double)nx * (ny + 1);
+    const double pts_geo = (double)mtot;                          // point arrays read once
+    const double pts_res = shared ? (double)B * mtot : (double)mtot;  // per-problem residuals
+    switch (kernel) {
+      case 0:
+        k_nufft_interp<T><<<dim3(interp_blocks(), B), 256, 0, s>>>(geo, g, gstride, nx, ny, inv_mm, c.st, kGateAll,
+                                                                   c.part, kQChiX, d_y2.as<cplx<T>>());
+        MF_LAUNCH_CK();
+        return B * G * cs + pts_geo * (8 + 2 * kTaps * ts + 24) + pts_res * cs;
+      case 1:
+        k_nufft_spread<T><<<dim3(ntiles, B), tile_r * tile_c, 0, s>>>(geo, d_y2.as<cplx<T>>(), g, gstride, nx, ny,
+                                                                      tile_r, tile_c, ntiles, c.st, kGateGrad);
+        MF_LAUNCH_CK();
+        return pts_geo * (8 + 2 * kTaps * ts) + pts_res * cs + B * G * cs;
+      case 2:
+        k_nufft_rows_fwd<T><<<dim3(cdiv(nx, rpc), B), 256, smem_rows, s>>>(
+            c.z, c.xstride, geo.e4, g, gstride, nx, ny, fh.dev, tw2h.as<cplx<T>>(), c.st, kGateAll, rpc);
+        MF_LAUNCH_CK();
+        return B * N * 8 + N * 8 + B * half_rows * cs;
+      case 3:
+        k_nufft_cols<T><<<dim3(cdiv(ny + 1, cpc), B), 256, smem_cols, s>>>(g, gstride, nx, ny, fcol.dev, -1, cpc, 1, 0,
+                                                                           c.st, kGateAll);
+        MF_LAUNCH_CK();
+        return B * (half_rows + G) * cs;
+      case 4:
+        k_nufft_cols<T><<<dim3(cdiv(ny + 1, cpc), B), 256, smem_cols, s>>>(g, gstride, nx, ny, fcol.dev, +1, cpc, 0, 1,
+                                                                           c.st, kGateGrad);
+        MF_LAUNCH_CK();
+        return B * (G + half_rows) * cs;
+      case 5: {
+        TsvFuse tf{c.z, c.prm, c.tsvNX, c.tsvNY};
+        k_nufft_rows_inv<T><<<dim3(cdiv(nx, rpc), B), 256, smem_rows, s>>>(
+            g, gstride, c.dfdx, c.xstride, geo.e4, nx, ny, inv_mm, fh.dev, tw2h.as<cplx<T>>(), tf, c.part, kQTsvZ,
+            c.st, kGateGrad, rpc);
+        MF_LAUNCH_CK();
+        return B * (half_rows * cs + 2 * N * 8) + N * 8;
+      }
+      default:
+        return -1;
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// gridded FFT operator
+// ---------------------------------------------------------------------------
+struct FftVarInput {
+  const int *u_idx, *v_idx;
+  const double *y_r, *y_i, *noise;
+  int M, NX, NY;
+};
+
+template <typename T> struct FftVarOp : Op {
+  Ctx& c;
+  int NX, NY, NYh, B;
+  DevMem d_mask, d_yf, d_H, tw2h;
+  FftHost<T> fh, fnx;
+  FftVarGeom geo{};
+  int rpc = 8, cpc = 8;
+  size_t smem_rows = 0, smem_cols = 0;
+  long hstride = 0;
+  double sqrtn = 0;
+
+  FftVarOp(Ctx& ctx, const FftVarInput& in) : c(ctx) {
+    NX = in.NX;
+    NY = in.NY;
+    B = ctx.B;
+    if (NY % 2 != 0 || NX < 2 || NY < 2) throw Error(MFISTA_ERR_ARG, "FFT variant needs an even NY >= 2");
+    NYh = NY / 2 + 1;
+    // idx2mat (:70-88) then full2half / fft_full2half (:50-68)
+    std::vector<double> mk_full((size_t)NX * NY, 0.0);
+    std::vector<double2> yf_full((size_t)NX * NY, make_double2(0.0, 0.0));
+    for (int i = 0; i < in.M; ++i) {
+      int u = in.u_idx[i], v = in.v_idx[i];
+      if (u < 0 || u >= NX || v < 0 || v >= NY) throw Error(MFISTA_ERR_ARG, "u_idx/v_idx outside the grid");
+      size_t e = (size_t)NY * u + v;
+      mk_full[e] = 1 / in.noise[i];
+      yf_full[e] = make_double2(in.y_r[i] / in.noise[i], in.y_i[i] / in.noise[i]);
+    }
+    std::vector<double> mh((size_t)NX * NYh);
+    std::vector<double2> yh((size_t)NX * NYh);
+    for (int i = 0; i < NX; ++i)
+      for (int j = 0; j < NYh; ++j) {
+        mh[(size_t)NYh * i + j] = mk_full[(size_t)NY * i + j];
+        yh[(size_t)NYh * i + j] = yf_full[(size_t)NY * i + j];
+      }
+    d_mask.upload(mh.data(), mh.size());
+    d_yf.upload(yh.data(), yh.size());
+    geo.mask_h = d_mask.as<double>();
+    geo.yf_h = d_yf.as<double2>();
+    geo.geo_stride = 0;
+    fh.init(NY / 2);
+    fnx.init(NX);
+    make_twiddles<T>(NY, tw2h);
+    hstride = (long)NX * NYh;
+    d_H.alloc(sizeof(cplx<T>) * (size_t)B * hstride);
+    sqrtn = sqrt((double)(NX * NY));
+    auto rows_smem = [&](int r) { return (size_t)2 * r * (NY / 2 + 1) * sizeof(cplx<T>); };
+    auto cols_smem = [&](int cc) { return (size_t)2 * cc * (NX + 1) * sizeof(cplx<T>); };
+    while (rpc > 1 && rows_smem(rpc) > 96 * 1024) rpc /= 2;
+    while (cpc > 1 && cols_smem(cpc) > 96 * 1024) cpc /= 2;
+    smem_rows = rows_smem(rpc);
+    smem_cols = cols_smem(cpc);
+    set_smem(k_fftv_rows_fwd<T>, smem_rows);
+    set_smem(k_fftv_rows_inv<T>, smem_rows);
+    set_smem(k_fftv_cols<T>, smem_cols);
+  }
+
+  void forward(cudaStream_t s, const double* src, int gate, int qchi, bool store) override {
+    cplx<T>* H = d_H.as<cplx<T>>();
+    k_fftv_rows_fwd<T><<<dim3(cdiv(NX, rpc), B), 256, smem_rows, s>>>(src, c.xstride, H, hstride, NX, NY, fh.dev,
+                                                                      tw2h.as<cplx<T>>(), c.st, gate, rpc);
+    MF_LAUNCH_CK();
+    k_fftv_cols<T><<<dim3(cdiv(NYh, cpc), B), 256, smem_cols, s>>>(H, hstride, NX, NYh, fnx.dev, -1, cpc, geo, sqrtn,
+                                                                   c.st, gate, c.part, qchi, store ? 1 : 0);
+    MF_LAUNCH_CK();
+  }
+
+  void adjoint(cudaStream_t s, const double* z_tsv, int qtsv) override {
+    cplx<T>* H = d_H.as<cplx<T>>();
+    k_fftv_cols<T><<<dim3(cdiv(NYh, cpc), B), 256, smem_cols, s>>>(H, hstride, NX, NYh, fnx.dev, +1, cpc, geo, sqrtn,
+                                                                   c.st, kGateGrad, c.part, -1, 0);
+    MF_LAUNCH_CK();
+    k_fftv_rows_inv<T><<<dim3(cdiv(NX, rpc), B), 256, smem_rows, s>>>(
+        H, hstride, c.dfdx, c.xstride, NX, NY, fh.dev, tw2h.as<cplx<T>>(), z_tsv, c.prm, c.tsvNX, c.tsvNY, c.part,
+        qtsv, c.st, kGateGrad, rpc);
+    MF_LAUNCH_CK();
+  }
+
+  int chi_slots() const override { return cdiv(NYh, cpc); }
+  int tsv_slots() const override { return cdiv(NX, rpc); }
+  double fscale() const override { return 0.25; }
+  int launches_forward() const override { return 2; }
+  int launches_adjoint() const override { return 2; }
+};
+
+// ---------------------------------------------------------------------------
+// dense DFT operator (FP64)
+// ---------------------------------------------------------------------------
+struct DftOp : Op {
+  Ctx& c;
+  DftGeom g{};
+  DevMem d_A, d_y, d_part, d_resid;
+  int B;
+
+  DftOp(Ctx& ctx, const double* A, const double* y, int M, int N) : c(ctx) {
+    B = ctx.B;
+    d_A.upload(A, (size_t)M * N);
+    d_y.upload(y, M);
+    g.A = d_A.as<double>();
+    g.y = d_y.as<double>();
+    g.M = M;
+    g.N = N;
+    g.chunk = 64;
+    g.nchunk = cdiv(N, g.chunk);
+    d_part.alloc(sizeof(double) * (size_t)B * g.nchunk * std::max(M, 1));
+    d_resid.alloc(sizeof(double) * (size_t)B * std::max(M, 1));
+    g.az_part = d_part.as<double>();
+    g.resid = d_resid.as<double>();
+  }
+
+  void forward(cudaStream_t s, const double* src, int gate, int qchi, bool store) override {
+    k_dft_az<<<dim3(std::max(1, cdiv(g.M, 256)), g.nchunk, B), 256, g.chunk * sizeof(double), s>>>(g, src, c.xstride,
+                                                                                                     c.st, gate);
+    MF_LAUNCH_CK();
+    k_dft_resid<<<dim3(std::max(1, cdiv(g.M, 256)), B), 256, 0, s>>>(g, c.st, gate, c.part, qchi, store ? 1 : 0);
+    MF_LAUNCH_CK();
+  }
+
+  void adjoint(cudaStream_t s, const double* z_tsv, int qtsv) override {
+    k_dft_atr<<<dim3(cdiv(g.N, 8), B), 256, 0, s>>>(g, c.dfdx, c.xstride, z_tsv, c.prm, c.tsvNX, c.tsvNY, c.st,
+                                                     kGateGrad, c.part, qtsv);
+    MF_LAUNCH_CK();
+  }
+
+  int chi_slots() const override { return std::max(1, cdiv(g.M, 256)); }
+  int tsv_slots() const override { return cdiv(g.N, 8); }
+  double fscale() const override { return 0.5; }
+  int launches_forward() const override { return 2; }
+  int launches_adjoint() const override { return 1; }
+};
+
+// ---------------------------------------------------------------------------
+// batched MFISTA driver
+// ---------------------------------------------------------------------------
+struct Solver {
+  Ctx ctx;
+  std::unique_ptr<Op> op;
+  int form = kFormTSV;
+  int precision = MFISTA_FP64;
+  int fgp_iter = 100;
+  int step_cap = 0;
+  DevMem d_x, d_z, d_xnew, d_dfdx, d_prm, d_st, d_part, d_out, d_box, d_fgp, d_steps;
+  unsigned long long step_budget = 0;
+  ImgDims dm{};
+  cudaStream_t stream = nullptr, cap_stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t body_graph = nullptr;  // host-loop fallback
+  cudaGraphExec_t body_exec = nullptr;
+  bool host_loop = false;
+  int* h_any = nullptr;
+  int* d_any = nullptr;
+  // FGP launch shape
+  int fgp_cs = 8, fgp_rpc = 0;
+  bool fgp_smem = true;
+  size_t fgp_smem_bytes = 0;
+  long fgp_scratch_stride = 0;
+  int per_step_launches = 0;
+  int fixed_launches = 0;
+  const float* box_ptr = nullptr;
+
+  Solver() {}
+  ~Solver() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (body_exec) cudaGraphExecDestroy(body_exec);
+    if (body_graph) cudaGraphDestroy(body_graph);
+    if (h_any) cudaFreeHost(h_any);
+    if (stream) cudaStreamDestroy(stream);
+    if (cap_stream) cudaStreamDestroy(cap_stream);
+  }
+
+  void init_common(int B, int N, int NX, int NY, int form_, int fgp_iter_, const float* box) {
+    ctx.B = B;
+    ctx.N = N;
+    ctx.xstride = N;
+    ctx.tsvNX = NX;
+    ctx.tsvNY = NY;
+    form = form_;
+    fgp_iter = fgp_iter_;
+    MF_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    MF_CK(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+    d_x.alloc(sizeof(double) * (size_t)B * N);
+    d_z.alloc(sizeof(double) * (size_t)B * N);
+    d_xnew.alloc(sizeof(double) * (size_t)B * N);
+    d_dfdx.alloc(sizeof(double) * (size_t)B * N);
+    d_prm.alloc(sizeof(ProbParams) * B);
+    d_st.alloc(sizeof(ProbState) * B);
+    d_out.alloc(sizeof(FinalOut) * B);
+    d_steps.alloc(2 * sizeof(unsigned long long));
+    ctx.x = d_x.as<double>();
+    ctx.z = d_z.as<double>();
+    ctx.xnew = d_xnew.as<double>();
+    ctx.dfdx = d_dfdx.as<double>();
+    ctx.prm = d_prm.as<ProbParams>();
+    ctx.st = d_st.as<ProbState>();
+    dm.N = N;
+    dm.NX = NX;
+    dm.NY = NY;
+    dm.xstride = N;
+    if (box) {
+      d_box.upload(box, N);
+      box_ptr = d_box.as<float>();
+    }
+    MF_CK(cudaHostAlloc((void**)&h_any, sizeof(int), cudaHostAllocMapped));
+    MF_CK(cudaHostGetDevicePointer((void**)&d_any, h_any, 0));
+  }
+
+  int img_blocks() const { return cdiv(ctx.N, 256); }
+
+  void finish_setup() {
+    int slots = std::max({op->chi_slots(), op->tsv_slots(), img_blocks(), 1});
+    d_part.alloc(sizeof(double) * (size_t)kNumQ * ctx.B * slots);
+    MF_CK(cudaMemset(d_part.p, 0, d_part.bytes));
+    ctx.part.p = d_part.as<double>();
+    ctx.part.slots = slots;
+    ctx.part.B = ctx.B;
+    if (form == kFormTV) setup_fgp();
+    per_step_launches = op->launches_forward() * 2 + op->launches_adjoint() + 3 + (form == kFormTV ? 1 : 0);
+    fixed_launches = 2 * (op->launches_forward() + 2) + 1;
+    const char* hl = getenv("MFISTA_HOST_LOOP");
+    host_loop = hl && hl[0] == '1';
+    build_graph();
+  }
+
+  template <typename K> int max_clusters(K kern, int cs, size_t smem) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs, 1, 1);
+    cfg.blockDim = dim3(256, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    return n;
+  }
+
+  template <typename K> void prep_fgp_kernel(K kern, int cs, size_t smem) {
+    if (cs > 8) MF_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    if (smem) MF_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
+
+  // Picks the FGP cluster shape: slabs in shared memory with 8 or 16 CTAs
+  // when they fit and such a cluster can be resident, else global slabs.
+  template <typename T> void pick_fgp_shape() {
+    int NX = ctx.tsvNX, NY = ctx.tsvNY;
+    const size_t limit = 200 * 1024;
+    for (int cs : {8, 16}) {
+      int rpc = cdiv(NY, cs);
+      size_t bytes = (size_t)6 * rpc * NX * sizeof(T);
+      if (bytes > limit) continue;
+      prep_fgp_kernel(k_fgp<T, true>, cs, bytes);
+      if (max_clusters(k_fgp<T, true>, cs, bytes) > 0) {
+        fgp_cs = cs;
+        fgp_rpc = rpc;
+        fgp_smem = true;
+        fgp_smem_bytes = bytes;
+        return;
+      }
+    }
+    fgp_cs = 8;
+    fgp_rpc = cdiv(NY, fgp_cs);
+    fgp_smem = false;
+    fgp_smem_bytes = 0;
+    prep_fgp_kernel(k_fgp<T, false>, fgp_cs, 0);
+    fgp_scratch_stride = (long)fgp_cs * 6 * fgp_rpc * NX * sizeof(T);
+    d_fgp.alloc((size_t)ctx.B * fgp_scratch_stride);
+  }
+
+  void setup_fgp() {
+    if (precision == MFISTA_FP32) pick_fgp_shape<float>();
+    else pick_fgp_shape<double>();
+  }
+
+  void launch_fgp(cudaStream_t s) {
+    FgpArgs a;
+    a.z = ctx.z;
+    a.dfdx = ctx.dfdx;
+    a.xnew = ctx.xnew;
+    a.xstride = ctx.xstride;
+    a.prm = ctx.prm;
+    a.st = ctx.st;
+    a.box = box_ptr;
+    a.NX = ctx.tsvNX;
+    a.NY = ctx.tsvNY;
+    a.iters = fgp_iter;
+    a.rows_per_cta = fgp_rpc;
+    a.scratch = d_fgp.p;
+    a.scratch_stride = fgp_scratch_stride;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(fgp_cs, ctx.B, 1);
+    cfg.blockDim = dim3(256, 1, 1);
+    cfg.dynamicSmemBytes = fgp_smem_bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = fgp_cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (precision == MFISTA_FP32) {
+      if (fgp_smem) MF_CK(cudaLaunchKernelEx(&cfg, k_fgp<float, true>, a));
+      else MF_CK(cudaLaunchKernelEx(&cfg, k_fgp<float, false>, a));
+    } else {
+      if (fgp_smem) MF_CK(cudaLaunchKernelEx(&cfg, k_fgp<double, true>, a));
+      else MF_CK(cudaLaunchKernelEx(&cfg, k_fgp<double, false>, a));
+    }
+  }
+
+  CtrlCfg ctrl_cfg(int mode) const {
+    CtrlCfg cfg;
+    memset(&cfg, 0, sizeof(cfg));
+    cfg.slots[kQChiZ] = op->chi_slots();
+    cfg.slots[kQChiX] = op->chi_slots();
+    cfg.slots[kQTsvZ] = form == kFormTSV ? op->tsv_slots() : 0;
+    cfg.slots[kQDq1] = img_blocks();
+    cfg.slots[kQDq2] = img_blocks();
+    cfg.slots[kQL1] = img_blocks();
+    cfg.slots[kQReg] = img_blocks();
+    cfg.slots[kQNact] = img_blocks();
+    cfg.fscale = op->fscale();
+    cfg.form = form;
+    cfg.mode = mode;
+    cfg.B = ctx.B;
+    cfg.steps = d_steps.as<unsigned long long>();
+    return cfg;
+  }
+
+  void launch_control(cudaStream_t s, int mode, cudaGraphConditionalHandle h, int set_handle) {
+    k_control<<<1, 1024, 0, s>>>(ctx.prm, ctx.st, ctx.part, ctrl_cfg(mode), d_out.as<FinalOut>(), h, set_handle,
+                                  d_any);
+    MF_LAUNCH_CK();
+  }
+
+  void enqueue_body(cudaStream_t s, cudaGraphConditionalHandle h, int set_handle) {
+    dim3 ig(img_blocks(), ctx.B);
+    // gradient at z (only problems that start a new outer iteration)
+    op->forward(s, ctx.z, kGateGrad, kQChiZ, true);
+    op->adjoint(s, form == kFormTSV ? ctx.z : nullptr, form == kFormTSV ? kQTsvZ : -1);
+    // trial point
+    if (form == kFormTSV) {
+      k_update_tsv<<<ig, 256, 0, s>>>(ctx.z, ctx.dfdx, ctx.xnew, dm, ctx.prm, ctx.st, box_ptr, ctx.part);
+      MF_LAUNCH_CK();
+    } else {
+      launch_fgp(s);
+      k_stats<<<ig, 256, 0, s>>>(ctx.xnew, ctx.z, ctx.dfdx, dm, ctx.prm, ctx.st, kGateTrial, form, 0, 1, ctx.part);
+      MF_LAUNCH_CK();
+    }
+    op->forward(s, ctx.xnew, kGateTrial, kQChiX, false);
+    launch_control(s, kCtrlStep, h, set_handle);
+    k_momentum<<<ig, 256, 0, s>>>(ctx.x, ctx.z, ctx.xnew, dm, ctx.st);
+    MF_LAUNCH_CK();
+  }
+
+  void build_graph() {
+    if (!host_loop) {
+      cudaError_t e = try_build_conditional();
+      if (e == cudaSuccess) return;
+      cudaGetLastError();
+      if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+      if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+      host_loop = true;
+    }
+    MF_CK(cudaStreamBeginCapture(cap_stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_body(cap_stream, 0, 0);
+    MF_CK(cudaStreamEndCapture(cap_stream, &body_graph));
+    MF_CK(cudaGraphInstantiate(&body_exec, body_graph, 0));
+  }
+
+  cudaError_t try_build_conditional() {
+    cudaError_t e;
+    if ((e = cudaGraphCreate(&graph, 0)) != cudaSuccess) return e;
+    cudaGraphConditionalHandle h;
+    if ((e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess) return e;
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    if ((e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp)) != cudaSuccess) return e;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if ((e = cudaStreamBeginCaptureToGraph(cap_stream, body, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+      return e;
+    try {
+      enqueue_body(cap_stream, h, 1);
+    } catch (...) {
+      cudaGraph_t tmp;
+      cudaStreamEndCapture(cap_stream, &tmp);
+      throw;
+    }
+    cudaGraph_t out;
+    if ((e = cudaStreamEndCapture(cap_stream, &out)) != cudaSuccess) return e;
+    return cudaGraphInstantiate(&exec, graph, 0);
+  }
+
+  // params: per problem; x0: [B*N] host (null = zeros); skip_loop: start
+  // from x0 and only compute the summary (reference early-return cases)
+  void upload_problems(const std::vector<ProbParams>& prm, const double* x0) {
+    MF_CK(cudaMemcpyAsync(ctx.prm, prm.data(), sizeof(ProbParams) * ctx.B, cudaMemcpyHostToDevice, stream));
+    size_t bytes = sizeof(double) * (size_t)ctx.B * ctx.N;
+    if (x0) MF_CK(cudaMemcpyAsync(ctx.x, x0, bytes, cudaMemcpyHostToDevice, stream));
+    else MF_CK(cudaMemsetAsync(ctx.x, 0, bytes, stream));
+    // device step budget: generous against the reference's own bound
+    // (maxiter outer iterations, each with at most maxiter trials)
+    long long mx = 1;
+    for (const ProbParams& p : prm) mx = std::max<long long>(mx, p.maxiter);
+    steps_host[0] = 0;
+    steps_host[1] = (unsigned long long)(mx * 64 + 4096);
+    MF_CK(cudaMemcpyAsync(d_steps.p, steps_host, sizeof(steps_host), cudaMemcpyHostToDevice, stream));
+  }
+  unsigned long long steps_host[2] = {0, 0};
+
+  // times one kernel alone: every problem active at the start of an outer
+  // iteration, `reps` launches between two events on the solver stream
+  void profile_kernel(int kernel, int reps, double& ms, double& bytes) {
+    std::vector<ProbState> st(ctx.B);
+    std::vector<ProbParams> prm(ctx.B);
+    MF_CK(cudaMemcpy(prm.data(), ctx.prm, sizeof(ProbParams) * ctx.B, cudaMemcpyDeviceToHost));
+    for (int b = 0; b < ctx.B; ++b) {
+      memset(&st[b], 0, sizeof(ProbState));
+      st[b].active = 1;
+      st[b].need_grad = 1;
+      st[b].c = prm[b].cinit > 0 ? prm[b].cinit : 1.0;
+    }
+    MF_CK(cudaMemcpy(ctx.st, st.data(), sizeof(ProbState) * ctx.B, cudaMemcpyHostToDevice));
+    auto one = [&]() -> double {
+      if (kernel == 6) {
+        dim3 ig(img_blocks(), ctx.B);
+        if (form == kFormTSV) {
+          k_update_tsv<<<ig, 256, 0, stream>>>(ctx.z, ctx.dfdx, ctx.xnew, dm, ctx.prm, ctx.st, box_ptr, ctx.part);
+          MF_LAUNCH_CK();
+        } else {
+          launch_fgp(stream);
+        }
+        return (double)ctx.B * ctx.N * 24.0;
+      }
+      return op->launch_single(stream, kernel);
+    };
+    bytes = one();
+    if (bytes < 0) throw Error(MFISTA_ERR_ARG, "no such kernel for this operator");
+    cudaEvent_t e0, e1;
+    MF_CK(cudaEventCreate(&e0));
+    MF_CK(cudaEventCreate(&e1));
+    MF_CK(cudaEventRecord(e0, stream));
+    for (int r = 0; r < reps; ++r) one();
+    MF_CK(cudaEventRecord(e1, stream));
+    MF_CK(cudaEventSynchronize(e1));
+    float t = 0;
+    MF_CK(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ms = t / reps;
+  }
+
+  long long steps_taken() {
+    unsigned long long h[2];
+    MF_CK(cudaMemcpy(h, d_steps.p, sizeof(h), cudaMemcpyDeviceToHost));
+    return (long long)h[0];
+  }
+
+  void enqueue_solve(bool skip_loop) {
+    dim3 ig(img_blocks(), ctx.B);
+    size_t bytes = sizeof(double) * (size_t)ctx.B * ctx.N;
+    MF_CK(cudaMemcpyAsync(ctx.z, ctx.x, bytes, cudaMemcpyDeviceToDevice, stream));
+    k_init_state<<<cdiv(ctx.B, 128), 128, 0, stream>>>(ctx.st, ctx.B, 0);
+    MF_LAUNCH_CK();
+    if (!skip_loop) {
+      op->forward(stream, ctx.x, kGateInit, kQChiX, false);
+      k_stats<<<ig, 256, 0, stream>>>(ctx.x, nullptr, nullptr, dm, ctx.prm, ctx.st, kGateInit, form, 0, 0, ctx.part);
+      MF_LAUNCH_CK();
+      launch_control(stream, kCtrlInit, 0, 0);
+      if (!host_loop) {
+        MF_CK(cudaGraphLaunch(exec, stream));
+      } else {
+        for (;;) {
+          for (int k = 0; k < 8; ++k) MF_CK(cudaGraphLaunch(body_exec, stream));
+          MF_CK(cudaStreamSynchronize(stream));
+          if (*(volatile int*)h_any == 0) break;
+        }
+      }
+    }
+    // summary at x (calc_result_*)
+    op->forward(stream, ctx.x, kGateAll, kQChiX, true);
+    k_stats<<<ig, 256, 0, stream>>>(ctx.x, nullptr, nullptr, dm, ctx.prm, ctx.st, kGateAll, form, 1, 0, ctx.part);
+    MF_LAUNCH_CK();
+    launch_control(stream, kCtrlFinal, 0, 0);
+  }
+
+  void fetch(double* xout, std::vector<FinalOut>& out) {
+    out.resize(ctx.B);
+    MF_CK(cudaMemcpyAsync(out.data(), d_out.p, sizeof(FinalOut) * ctx.B, cudaMemcpyDeviceToHost, stream));
+    if (xout)
+      MF_CK(cudaMemcpyAsync(xout, ctx.x, sizeof(double) * (size_t)ctx.B * ctx.N, cudaMemcpyDeviceToHost, stream));
+    MF_CK(cudaStreamSynchronize(stream));
+  }
+};
+
+}  // namespace mf

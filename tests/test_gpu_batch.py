@@ -1,0 +1,108 @@
+"""Batched solves: per-problem state and masks on the device.
+
+Every problem of an FP64 batch must reproduce the single-problem drop-in
+solve with the same parameters (the kernels never mix problems, so the
+arithmetic is identical); the FP32 form is checked against FP64.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _single(si, c0, lam1, lts, maxiter, nonneg=1):
+    return si.imaging_core_nufft(c0["u"], c0["v"], c0["vis_r"], c0["vis_i"], c0["vis_std"], 64, 64,
+                                 maxiter, 1e-5, lam1, 0.0, lts, float(c0["cinit"]), nonneg_flag=nonneg)
+
+
+def _problems(c0, scales, maxiter):
+    lam1 = float(c0["lam1"])
+    return [dict(lambda_l1=lam1 * s, lambda_tsv=lam1 * 1e-3 * s, cinit=float(c0["cinit"]),
+                 maxiter=maxiter, nonneg_flag=1) for s in scales]
+
+
+def test_shared_geometry_batch_equals_single_solves(gpulib, c0):
+    scales = [0.3, 1.0, 4.0]
+    probs = _problems(c0, scales, 120)
+    X, R = gpulib.nufft_batch(c0["u"], c0["v"], c0["vis_r"], c0["vis_i"], c0["vis_std"], 64, 64,
+                              probs, 1e-5)
+    for b, p in enumerate(probs):
+        x, r = _single(gpulib, c0, p["lambda_l1"], p["lambda_tsv"], 120)
+        assert R[b]["ITER"] == r["ITER"]
+        assert rel(X[b], x) < 1e-13
+        assert abs(R[b]["finalcost"] - r["finalcost"]) <= 1e-13 * r["finalcost"]
+
+
+def test_uneven_geometry_batch_equals_single_solves(gpulib, c0):
+    """Three problems with 2016, 1200 and 700 points in one launch."""
+    m = c0["u"].size
+    sizes = [m, 1200, 700]
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    cat = lambda a: np.concatenate([a[:s] for s in sizes])
+    probs = _problems(c0, [1.0, 1.0, 1.0], 100)
+    X, R = gpulib.nufft_batch(cat(c0["u"]), cat(c0["v"]), cat(c0["vis_r"]), cat(c0["vis_i"]),
+                              cat(c0["vis_std"]), 64, 64, probs, 1e-5, pt_off=off)
+    for b, s in enumerate(sizes):
+        x, r = gpulib.imaging_core_nufft(c0["u"][:s], c0["v"][:s], c0["vis_r"][:s], c0["vis_i"][:s],
+                                         c0["vis_std"][:s], 64, 64, 100, 1e-5, probs[b]["lambda_l1"], 0.0,
+                                         probs[b]["lambda_tsv"], probs[b]["cinit"])
+        assert R[b]["ITER"] == r["ITER"] and R[b]["M"] == s // 2
+        assert rel(X[b], x) < 1e-13
+
+
+def test_fp32_form_against_fp64(gpulib, c0):
+    probs = _problems(c0, [0.5, 1.0, 2.0, 8.0], 150)
+    args = (c0["u"], c0["v"], c0["vis_r"], c0["vis_i"], c0["vis_std"], 64, 64, probs, 1e-5)
+    X64, R64 = gpulib.nufft_batch(*args)
+    X32, R32 = gpulib.nufft_batch(*args, precision=gpulib.FP32)
+    for b in range(len(probs)):
+        assert rel(X32[b], X64[b]) < 1e-3
+        assert abs(R32[b]["finalcost"] - R64[b]["finalcost"]) <= 1e-6 * R64[b]["finalcost"]
+
+
+def test_plan_reuse_is_deterministic(gpulib, c0):
+    probs = _problems(c0, [0.7, 1.3], 80)
+    plan = gpulib.Plan(c0["u"], c0["v"], c0["vis_r"], c0["vis_i"], c0["vis_std"], 64, 64, 2)
+    plan.set_problems(probs, 1e-5)
+    plan.run()
+    X1, R1 = plan.fetch()
+    plan.set_problems(probs, 1e-5)
+    plan.run()
+    X2, R2 = plan.fetch()
+    assert np.array_equal(X1, X2)
+    assert [r["ITER"] for r in R1] == [r["ITER"] for r in R2]
+    assert plan.kernel_launches > 80
+    plan.close()
+
+
+def test_tv_batch_equals_single(gpulib, c0):
+    lam1 = float(c0["lam1"])
+    probs = [dict(lambda_l1=lam1, lambda_tv=5e-3 * lam1 * s, cinit=float(c0["cinit"]), maxiter=30,
+                  nonneg_flag=1) for s in (1.0, 3.0)]
+    X, R = gpulib.nufft_batch(c0["u"], c0["v"], c0["vis_r"], c0["vis_i"], c0["vis_std"], 64, 64, probs,
+                              1e-5)
+    for b, p in enumerate(probs):
+        x, r = gpulib.imaging_core_nufft(c0["u"], c0["v"], c0["vis_r"], c0["vis_i"], c0["vis_std"], 64, 64,
+                                         30, 1e-5, lam1, p["lambda_tv"], 0.0, p["cinit"])
+        assert R[b]["ITER"] == r["ITER"]
+        assert rel(X[b], x) < 1e-13
+
+
+def test_nan_visibility_stops_with_status(gpulib, c0):
+    """NaN data never passes the backtracking test; the problem stops with
+    MFISTA_ERR_NONFINITE (5) instead of retrying maxiter times per iteration."""
+    vr = c0["vis_r"].copy()
+    vr[3] = np.nan
+    probs = _problems(c0, [1.0], 1000)
+    with pytest.raises(gpulib.MfistaError) as e:
+        gpulib.nufft_batch(c0["u"], c0["v"], vr, c0["vis_i"], c0["vis_std"], 64, 64, probs, 1e-5)
+    assert e.value.status == 5
+
+
+def test_batch_rejects_mixed_regularisers(gpulib, c0):
+    probs = _problems(c0, [1.0], 10)
+    probs[0]["lambda_tv"] = 1.0
+    with pytest.raises(gpulib.MfistaError):
+        gpulib.nufft_batch(c0["u"], c0["v"], c0["vis_r"], c0["vis_i"], c0["vis_std"], 64, 64, probs, 1e-5)
