@@ -98,6 +98,11 @@ enum mfista_status {
   MFISTA_ERR_STEPCAP = 6     /* device step budget exhausted: problem stopped */
 };
 
+/* Selects the CUDA device used by this thread's subsequent calls (the
+ * library carries its own CUDA runtime, so a device chosen through another
+ * runtime, e.g. a framework's, does not carry over). */
+int mfista_set_device(int device);
+
 /* Status / message of the last call made by this thread. */
 int mfista_last_status(void);
 const char *mfista_last_error(void);
@@ -167,6 +172,9 @@ void *mfista_plan_stream(mfista_plan plan);          /* cudaStream_t */
 int mfista_plan_profile(mfista_plan plan, int kernel, int reps, double *ms_per_launch,
                         double *bytes_per_launch);
 int mfista_plan_kernel_launches(mfista_plan plan);   /* kernels per solve, last run */
+/* 1 when the plan iterates with a device-side conditional WHILE graph node,
+ * 0 when it fell back to relaunching the step graph from the host. */
+int mfista_plan_device_loop(mfista_plan plan);
 void mfista_plan_destroy(mfista_plan plan);
 
 /* Operators of the NUFFT variant, as the C++ reference exports them

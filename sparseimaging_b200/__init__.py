@@ -22,7 +22,7 @@ from .build import LIB
 __all__ = ["RESULT", "Problem", "MfistaError", "lib", "mfista_imaging_core_nufft",
            "mfista_imaging_core_fft", "mfista_imaging_core_dft", "imaging_core_nufft",
            "imaging_core_fft", "imaging_core_dft", "nufft_batch", "Plan", "nufft_forward",
-           "nufft_adjoint", "fgp_prox", "nufft_lipschitz", "last_status", "last_error", "set_fgp_iter",
+           "nufft_adjoint", "fgp_prox", "nufft_lipschitz", "last_status", "last_error", "set_fgp_iter", "set_device",
            "FP64", "FP32"]
 
 FP64 = 64
@@ -72,6 +72,8 @@ def lib():
         L = C.CDLL(LIB)
         L.mfista_last_error.restype = C.c_char_p
         L.mfista_last_status.restype = C.c_int
+        L.mfista_set_device.restype = C.c_int
+        L.mfista_set_device.argtypes = [C.c_int]
         L.mfista_set_fgp_iter.restype = C.c_int
         L.mfista_set_fgp_iter.argtypes = [C.c_int]
         L.mfista_imaging_core_nufft.restype = None
@@ -104,6 +106,8 @@ def lib():
         L.mfista_plan_fetch.argtypes = [C.c_void_p, _dp, C.POINTER(RESULT)]
         L.mfista_plan_stream.restype = C.c_void_p
         L.mfista_plan_stream.argtypes = [C.c_void_p]
+        L.mfista_plan_device_loop.restype = C.c_int
+        L.mfista_plan_device_loop.argtypes = [C.c_void_p]
         L.mfista_plan_kernel_launches.restype = C.c_int
         L.mfista_plan_kernel_launches.argtypes = [C.c_void_p]
         L.mfista_plan_profile.restype = C.c_int
@@ -121,6 +125,11 @@ def lib():
         L.mfista_nufft_lipschitz.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, _dp]
         _lib = L
     return _lib
+
+
+def set_device(device):
+    """CUDA device for this thread's subsequent calls."""
+    _check(lib().mfista_set_device(int(device)))
 
 
 def set_fgp_iter(n):
@@ -322,6 +331,10 @@ class Plan:
     @property
     def stream(self):
         return lib().mfista_plan_stream(self.h)
+
+    @property
+    def device_loop(self):
+        return bool(lib().mfista_plan_device_loop(self.h))
 
     @property
     def kernel_launches(self):

@@ -19,6 +19,7 @@ thread_local int g_fgp_iter = 100;  // FGPITER, c/mfista.h:38
 void set_ok() {
   g_status = MFISTA_OK;
   g_msg.clear();
+  cudaGetLastError();  // do not inherit a launch error of an earlier call
 }
 
 int fail(int st, const std::string& m, bool print) {
@@ -83,6 +84,12 @@ void run_single(MakeOp make_op, int N, int NX, int NY, int form, const float* bo
 }  // namespace
 
 extern "C" int mfista_last_status(void) { return g_status; }
+extern "C" int mfista_set_device(int device) {
+  set_ok();
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(MFISTA_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e), false);
+  return MFISTA_OK;
+}
 extern "C" int mfista_set_fgp_iter(int n) {
   if (n < 1) return -1;
   int old = g_fgp_iter;
@@ -377,6 +384,7 @@ extern "C" int mfista_plan_profile(mfista_plan P, int kernel, int reps, double* 
   }
 }
 extern "C" int mfista_plan_kernel_launches(mfista_plan P) { return P ? P->launches : 0; }
+extern "C" int mfista_plan_device_loop(mfista_plan P) { return P && !P->S->host_loop ? 1 : 0; }
 extern "C" void mfista_plan_destroy(mfista_plan P) { delete P; }
 
 extern "C" int mfista_nufft_batch(const double* u_dx, const double* v_dy, const double* vis_r, const double* vis_i,

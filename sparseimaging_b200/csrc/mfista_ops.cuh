@@ -220,7 +220,7 @@ __device__ __forceinline__ double warp_partial_sum(const double* p, int n, int l
   return warp_sum(s);
 }
 
-__global__ void k_control(const ProbParams* __restrict__ prm, ProbState* __restrict__ st, Partials part,
+__global__ void __launch_bounds__(256) k_control(const ProbParams* __restrict__ prm, ProbState* __restrict__ st, Partials part,
                           CtrlCfg cfg, FinalOut* __restrict__ out, cudaGraphConditionalHandle handle,
                           int set_handle, int* __restrict__ any_active) {
   __shared__ int s_any, s_cap;

@@ -724,7 +724,7 @@ struct Solver {
   }
 
   void launch_control(cudaStream_t s, int mode, cudaGraphConditionalHandle h, int set_handle) {
-    k_control<<<1, 1024, 0, s>>>(ctx.prm, ctx.st, ctx.part, ctrl_cfg(mode), d_out.as<FinalOut>(), h, set_handle,
+    k_control<<<1, 256, 0, s>>>(ctx.prm, ctx.st, ctx.part, ctrl_cfg(mode), d_out.as<FinalOut>(), h, set_handle,
                                   d_any);
     MF_LAUNCH_CK();
   }

@@ -74,6 +74,7 @@ def test_plan_reuse_is_deterministic(gpulib, c0):
     assert np.array_equal(X1, X2)
     assert [r["ITER"] for r in R1] == [r["ITER"] for r in R2]
     assert plan.kernel_launches > 80
+    assert plan.device_loop, "conditional WHILE graph node not in use"
     plan.close()
 
 
