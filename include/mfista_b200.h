@@ -146,6 +146,13 @@ int mfista_nufft_batch(const double *u_dx, const double *v_dy, const double *vis
                        int fgp_iter, const double *xinit, double *xout,
                        struct RESULT *results);
 
+/* Batched DFT solve (B problems sharing the column-major M x N matrix A and
+ * the data y, e.g. a lambda grid): A z and A^T r run as GEMMs over the
+ * batch.  eps is used raw, as mfista_imaging_core_dft does.  precision: 64. */
+int mfista_dft_batch(const double *y, const double *A, int M, int N, int NX, int NY, int B,
+                     const struct mfista_problem *problems, double eps, int precision,
+                     int fgp_iter, const double *xinit, double *xout, struct RESULT *results);
+
 /* Device-resident plan of a batched NUFFT solve.  Creation uploads the
  * geometry and visibilities once and builds the CUDA graph; mfista_plan_run
  * enqueues one whole batched solve on the plan's stream without waiting;
@@ -172,6 +179,8 @@ void *mfista_plan_stream(mfista_plan plan);          /* cudaStream_t */
 int mfista_plan_profile(mfista_plan plan, int kernel, int reps, double *ms_per_launch,
                         double *bytes_per_launch);
 int mfista_plan_kernel_launches(mfista_plan plan);   /* kernels per solve, last run */
+/* Per-problem status of the last fetched solve (enum mfista_status values). */
+int mfista_plan_statuses(mfista_plan plan, int *status_out);
 /* 1 when the plan iterates with a device-side conditional WHILE graph node,
  * 0 when it fell back to relaunching the step graph from the host. */
 int mfista_plan_device_loop(mfista_plan plan);

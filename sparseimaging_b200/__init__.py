@@ -21,7 +21,7 @@ from .build import LIB
 
 __all__ = ["RESULT", "Problem", "MfistaError", "lib", "mfista_imaging_core_nufft",
            "mfista_imaging_core_fft", "mfista_imaging_core_dft", "imaging_core_nufft",
-           "imaging_core_fft", "imaging_core_dft", "nufft_batch", "Plan", "nufft_forward",
+           "imaging_core_fft", "imaging_core_dft", "nufft_batch", "dft_batch", "Plan", "nufft_forward",
            "nufft_adjoint", "fgp_prox", "nufft_lipschitz", "last_status", "last_error", "set_fgp_iter", "set_device",
            "FP64", "FP32"]
 
@@ -95,6 +95,10 @@ def lib():
         L.mfista_nufft_batch.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, C.c_int, C.c_int, C.c_int,
                                          C.c_int, C.c_int, C.POINTER(Problem), C.c_double, C.c_int,
                                          C.c_int, _dp, _dp, C.POINTER(RESULT)]
+        L.mfista_dft_batch.restype = C.c_int
+        L.mfista_dft_batch.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.POINTER(Problem), C.c_double, C.c_int, C.c_int, _dp, _dp,
+                                       C.POINTER(RESULT)]
         L.mfista_nufft_plan_create.restype = C.c_void_p
         L.mfista_nufft_plan_create.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, C.c_int, C.c_int,
                                                C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
@@ -106,6 +110,8 @@ def lib():
         L.mfista_plan_fetch.argtypes = [C.c_void_p, _dp, C.POINTER(RESULT)]
         L.mfista_plan_stream.restype = C.c_void_p
         L.mfista_plan_stream.argtypes = [C.c_void_p]
+        L.mfista_plan_statuses.restype = C.c_int
+        L.mfista_plan_statuses.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
         L.mfista_plan_device_loop.restype = C.c_int
         L.mfista_plan_device_loop.argtypes = [C.c_void_p]
         L.mfista_plan_kernel_launches.restype = C.c_int
@@ -291,6 +297,22 @@ def nufft_batch(u_dx, v_dy, vis_r, vis_i, vis_std, nx, ny, problems, eps, precis
     return xo.reshape(B, n), [r.as_dict() for r in res]
 
 
+def dft_batch(y, A, nx, ny, problems, eps, xinit=None, fgp_iter=100):
+    """Solves len(problems) DFT problems sharing A (logical (M, N)) and y."""
+    A = np.asarray(A, np.float64)
+    m, n = A.shape
+    Af = np.asfortranarray(A)
+    yy = _d(y)
+    B = len(problems)
+    xi = None if xinit is None else _d(xinit)
+    xo = np.zeros(B * n)
+    res = (RESULT * B)()
+    st = lib().mfista_dft_batch(_p(yy), Af.ctypes.data_as(_dp), m, n, nx, ny, B, _problems(problems), eps,
+                                FP64, fgp_iter, _p(xi), _p(xo), res)
+    _check(st)
+    return xo.reshape(B, n), [r.as_dict() for r in res]
+
+
 class Plan:
     """Device-resident batched NUFFT plan (geometry uploaded once)."""
 
@@ -316,11 +338,22 @@ class Plan:
     def run(self):
         _check(lib().mfista_plan_run(self.h))
 
-    def fetch(self, want_x=True):
+    def fetch(self, want_x=True, check=True):
+        """(xout [B, N] or None, RESULT dicts).  check=False returns the
+        results of problems that stopped with a status instead of raising;
+        each dict then carries its own 'status'."""
         xo = np.zeros(self.B * self.n) if want_x else None
         res = (RESULT * self.B)()
-        _check(lib().mfista_plan_fetch(self.h, _p(xo), res))
-        return (None if xo is None else xo.reshape(self.B, self.n)), [r.as_dict() for r in res]
+        st = lib().mfista_plan_fetch(self.h, _p(xo), res)
+        if check:
+            _check(st)
+        out = [r.as_dict() for r in res]
+        if not check:
+            stat = (C.c_int * self.B)()
+            lib().mfista_plan_statuses(self.h, stat)
+            for d, s in zip(out, stat):
+                d["status"] = int(s)
+        return (None if xo is None else xo.reshape(self.B, self.n)), out
 
     def profile(self, kernel, reps=20):
         """(ms per launch, algorithmic bytes per launch) of one operator kernel."""

@@ -50,7 +50,7 @@ constexpr int kCostRing = 64;    // holds cost[iter - TD .. iter]
 // per-problem solver state (device resident)
 // ---------------------------------------------------------------------------
 enum Form { kFormTSV = 0, kFormTV = 1 };
-enum Gate { kGateInit = 0, kGateGrad = 1, kGateTrial = 2, kGateFinal = 3, kGateAll = 4 };
+enum Gate { kGateInit = 0, kGateGrad = 1, kGateTrial = 2, kGateFinal = 3, kGateAll = 4, kGateRefresh = 5 };
 
 struct ProbParams {
   double lambda_l1, lambda_tv, lambda_tsv;
@@ -80,7 +80,7 @@ struct ProbState {
   int take_x;     // accepted step is a monotone improvement: x = xnew
   int iters_out;  // RESULT.ITER once finished
   int status;     // 0 ok; nonzero = error (see mfista_status_*)
-  int pad_;
+  int refresh;    // FP32 form: recompute the FP64 anchor model in this step
 };
 
 // reduction quantities written as per-CTA partials
@@ -107,6 +107,7 @@ __device__ __forceinline__ bool gate_ok(const ProbState& s, int gate) {
   switch (gate) {
     case kGateGrad: return s.active && s.need_grad;
     case kGateTrial: return s.active != 0;
+    case kGateRefresh: return s.active && s.need_grad && s.refresh;
     default: return true;
   }
 }

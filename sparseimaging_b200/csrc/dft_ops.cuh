@@ -92,3 +92,135 @@ __global__ void k_dft_atr(DftGeom g, double* __restrict__ dall, long xstride, co
 }
 
 }  // namespace mf
+
+// ===========================================================================
+// Batched DFT (B problems share A): A Z and A^T R as register-blocked FP64
+// GEMMs with split-K; each CTA computes a 64 x 64 (rows x problems) tile.
+// Results are per-K-chunk partials summed in a fixed order afterwards, so
+// the batched path is deterministic like the GEMV path.
+// ===========================================================================
+namespace mf {
+
+constexpr int kGT = 64;   // tile edge (rows and problems)
+constexpr int kGK = 16;   // K step staged in shared memory
+
+// az_part[b][chunk][m] = sum_{n in chunk} A[m + n M] z_b[n]
+__global__ void __launch_bounds__(256) k_dft_az_gemm(DftGeom g, const double* __restrict__ zall, long xstride,
+                                                     const ProbState* __restrict__ st, int gate, int B) {
+  __shared__ double sA[kGK][kGT + 1];
+  __shared__ double sZ[kGK][kGT + 1];
+  const int m0 = blockIdx.x * kGT, b0 = blockIdx.z * kGT, c = blockIdx.y;
+  const int n0 = c * g.chunk, n1 = min(g.N, n0 + g.chunk);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16 threads, 4 x 4 outputs each
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (int k0 = n0; k0 < n1; k0 += kGK) {
+    for (int t = threadIdx.x; t < kGK * kGT; t += 256) {
+      int kk = t / kGT, r = t - kk * kGT;
+      int n = k0 + kk, m = m0 + r, b = b0 + r;
+      sA[kk][r] = (n < n1 && m < g.M) ? g.A[(size_t)n * g.M + m] : 0.0;
+      bool ok = n < n1 && b < B && gate_ok(st[b], gate);
+      sZ[kk][r] = ok ? zall[(size_t)b * xstride + n] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kGK; ++kk) {
+      double a[4], z[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = sA[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) z[j] = sZ[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * z[j];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    int b = b0 + tx + 16 * j;
+    if (b >= B || !gate_ok(st[b], gate)) continue;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      int m = m0 + ty + 16 * i;
+      if (m < g.M) g.az_part[((size_t)b * g.nchunk + c) * g.M + m] = acc[i][j];
+    }
+  }
+}
+
+// atr_part[b][chunk][n] = sum_{m in chunk} A[m + n M] r_b[m]
+__global__ void __launch_bounds__(256) k_dft_atr_gemm(DftGeom g, double* __restrict__ atr_part, int mchunk,
+                                                      int nmchunk, const ProbState* __restrict__ st, int gate,
+                                                      int B) {
+  __shared__ double sA[kGK][kGT + 1];
+  __shared__ double sR[kGK][kGT + 1];
+  const int nn0 = blockIdx.x * kGT, b0 = blockIdx.z * kGT, c = blockIdx.y;
+  const int ms = c * mchunk, me = min(g.M, ms + mchunk);
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (int k0 = ms; k0 < me; k0 += kGK) {
+    // A is column-major: 16 consecutive rows of column n are contiguous
+    for (int t = threadIdx.x; t < kGK * kGT; t += 256) {
+      int r = t / kGK, kk = t - r * kGK;
+      int m = k0 + kk, n = nn0 + r, b = b0 + r;
+      sA[kk][r] = (m < me && n < g.N) ? g.A[(size_t)n * g.M + m] : 0.0;
+      bool ok = m < me && b < B && gate_ok(st[b], gate);
+      sR[kk][r] = ok ? g.resid[(size_t)b * g.M + m] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kGK; ++kk) {
+      double a[4], r[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = sA[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) r[j] = sR[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * r[j];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    int b = b0 + tx + 16 * j;
+    if (b >= B || !gate_ok(st[b], gate)) continue;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      int n = nn0 + ty + 16 * i;
+      if (n < g.N) atr_part[((size_t)b * nmchunk + c) * g.N + n] = acc[i][j];
+    }
+  }
+}
+
+// dfdx[n] = beta dTSV(z)[n] + sum_chunks atr_part[b][c][n]
+__global__ void k_dft_atr_finish(DftGeom g, const double* __restrict__ atr_part, int nmchunk,
+                                 double* __restrict__ dall, long xstride, const double* __restrict__ zall,
+                                 const ProbParams* __restrict__ prm, int tsvNX, int tsvNY,
+                                 const ProbState* __restrict__ st, int gate) {
+  int b = blockIdx.y;
+  if (!gate_ok(st[b], gate)) return;
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= g.N) return;
+  double s = 0.0;
+  for (int c = 0; c < nmchunk; ++c) s += atr_part[((size_t)b * nmchunk + c) * g.N + n];
+  const ProbParams& pp = prm[b];
+  double* d = dall + (size_t)b * xstride;
+  if (zall != nullptr && pp.lambda_tsv > 0.0) {
+    const double* z = zall + (size_t)b * xstride;
+    d[n] = dtsv_at(z, n, tsvNX, tsvNY) * (-pp.lambda_tsv) + s;
+  } else {
+    d[n] = s;
+  }
+}
+
+}  // namespace mf

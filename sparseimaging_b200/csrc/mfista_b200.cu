@@ -260,6 +260,7 @@ struct mfista_plan_s {
   std::vector<ProbParams> prm;
   double comp_time = 0, t_start = 0;
   int launches = 0;
+  std::vector<int> statuses;
 };
 
 extern "C" mfista_plan mfista_nufft_plan_create(const double* u_dx, const double* v_dy, const double* vis_r,
@@ -281,7 +282,10 @@ extern "C" mfista_plan mfista_nufft_plan_create(const double* u_dx, const double
     S.precision = precision;
     S.init_common(B, Nx * Ny, Nx, Ny, P->form, fgp_iter, nullptr);
     NufftInput in{u_dx, v_dy, vis_r, vis_i, vis_std, pt_off, shared_geometry, M, Nx, Ny};
-    if (precision == MFISTA_FP32) S.op.reset(new NufftOp<float>(S.ctx, in));
+    // FP32 operators carry an FP64 defect correction unless disabled
+    const char* nc = getenv("MFISTA_FP32_NO_CORRECTION");
+    bool correct = !(nc && nc[0] == '1');
+    if (precision == MFISTA_FP32) S.op.reset(new NufftOp<float>(S.ctx, in, correct));
     else S.op.reset(new NufftOp<double>(S.ctx, in));
     S.finish_setup();
     P->m_of.resize(B);
@@ -352,7 +356,9 @@ extern "C" int mfista_plan_fetch(mfista_plan P, double* xout, struct RESULT* res
     long long steps = P->S->steps_taken();
     P->launches = (int)(P->S->fixed_launches + steps * P->S->per_step_launches);
     int worst = 0;
+    P->statuses.assign(P->B, 0);
     for (int b = 0; b < P->B; ++b) {
+      P->statuses[b] = o[b].status;
       const ProbParams& p = P->prm[b];
       if (results)
         fill_result(&results[b], o[b], P->m_of[b] / 2, (double)P->m_of[b], P->Nx, P->Ny, P->Nx * P->Ny, p.lambda_l1,
@@ -384,6 +390,11 @@ extern "C" int mfista_plan_profile(mfista_plan P, int kernel, int reps, double* 
   }
 }
 extern "C" int mfista_plan_kernel_launches(mfista_plan P) { return P ? P->launches : 0; }
+extern "C" int mfista_plan_statuses(mfista_plan P, int* status_out) {
+  if (!P) return MFISTA_ERR_ARG;
+  for (int b = 0; b < P->B; ++b) status_out[b] = b < (int)P->statuses.size() ? P->statuses[b] : 0;
+  return MFISTA_OK;
+}
 extern "C" int mfista_plan_device_loop(mfista_plan P) { return P && !P->S->host_loop ? 1 : 0; }
 extern "C" void mfista_plan_destroy(mfista_plan P) { delete P; }
 
@@ -404,6 +415,52 @@ extern "C" int mfista_nufft_batch(const double* u_dx, const double* v_dy, const 
   g_status = keep;
   g_msg = msg;
   return st;
+}
+
+extern "C" int mfista_dft_batch(const double* y, const double* A, int M, int N, int NX, int NY, int B,
+                                const struct mfista_problem* problems, double eps, int precision, int fgp_iter,
+                                const double* xinit, double* xout, struct RESULT* results) {
+  set_ok();
+  try {
+    if (B < 1) throw Error(MFISTA_ERR_ARG, "B must be >= 1");
+    if (precision != MFISTA_FP64) throw Error(MFISTA_ERR_ARG, "the batched DFT runs in FP64");
+    int form = problems[0].lambda_tv != 0 ? kFormTV : kFormTSV;
+    std::vector<ProbParams> prm(B);
+    for (int b = 0; b < B; ++b) {
+      const mfista_problem& q = problems[b];
+      if (q.lambda_tv != 0 && q.lambda_tsv != 0) throw Error(MFISTA_ERR_BOTH_REG, "lambda_tv and lambda_tsv both non-zero");
+      if ((form == kFormTV) != (q.lambda_tv != 0)) throw Error(MFISTA_ERR_ARG, "mixed TV / TSV problems");
+      if (form == kFormTSV && q.nonneg_flag != 0 && q.nonneg_flag != 1)
+        throw Error(MFISTA_ERR_ARG, "nonneg_flag must be 0 or 1");
+      if (q.maxiter < 0) throw Error(MFISTA_ERR_ARG, "maxiter must be >= 0");
+      prm[b] = ProbParams{q.lambda_l1, q.lambda_tv, q.lambda_tsv, q.cinit, eps, q.maxiter, q.nonneg_flag, 0, 0,
+                          q.target_cost};
+    }
+    Solver S;
+    S.precision = MFISTA_FP64;
+    S.init_common(B, N, NX, NY, form, fgp_iter, nullptr);
+    S.op.reset(new DftOp(S.ctx, A, y, M, N));
+    S.finish_setup();
+    double t0 = now_s();
+    S.upload_problems(prm, xinit);
+    S.enqueue_solve(false);
+    std::vector<FinalOut> o;
+    S.fetch(xout, o);
+    double ct = now_s() - t0;
+    int worst = 0;
+    for (int b = 0; b < B; ++b) {
+      if (results) {
+        fill_result(&results[b], o[b], M, (double)M, NX, NY, N, prm[b].lambda_l1, prm[b].lambda_tv,
+                    prm[b].lambda_tsv, prm[b].maxiter, prm[b].nonneg, ct, false, prm[b].cinit);
+        results[b].residual = nullptr;
+      }
+      if (o[b].status) worst = o[b].status;
+    }
+    if (worst) return fail(worst, "a problem stopped early (status " + std::to_string(worst) + ")", false);
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -70,12 +70,16 @@ struct ImgDims {
 // ---------------------------------------------------------------------------
 // TSV form trial step (c/mfista_nufft_lib.c:684-700):
 //   xtmp = dfdx/c + z ; xnew = soft_th(xtmp, lambda_l1/c)
-// fused with the Q-model dot products (calc_Q_part), |xnew|_1 and TSV(xnew).
+// fused with the Q-model dot products (calc_Q_part), |xnew|_1, TSV(xnew) and
+// TSV(z).  TSV(z) (for Qcore) and TSV(xnew) (for F) go through the same
+// decomposition and summation tree, so that xnew == z gives F == Q exactly,
+// as the reference's single TSV() does; two different reduction orders let
+// rounding fail the backtracking test forever once the step is tiny.
 // ---------------------------------------------------------------------------
 __global__ void k_update_tsv(const double* __restrict__ zall, const double* __restrict__ dall,
                              double* __restrict__ xnall, ImgDims dm, const ProbParams* __restrict__ prm,
                              const ProbState* __restrict__ st, const float* __restrict__ box, Partials part) {
-  __shared__ double sh[4 * 32];
+  __shared__ double sh[5 * 32];
   int b = blockIdx.y;
   if (!gate_ok(st[b], kGateTrial)) return;
   const ProbParams p = prm[b];
@@ -86,7 +90,7 @@ __global__ void k_update_tsv(const double* __restrict__ zall, const double* __re
   const double* d = dall + (size_t)b * dm.xstride;
   double* xn = xnall + (size_t)b * dm.xstride;
   const float* bx = p.box_flag == 1 ? box : nullptr;
-  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f < dm.N) {
     double xv = prox_l1(d[f] * cinv + z[f], eta, p.nonneg, bx, f);
@@ -105,14 +109,16 @@ __global__ void k_update_tsv(const double* __restrict__ zall, const double* __re
         double o = prox_l1(d[f + dm.NX] * cinv + z[f + dm.NX], eta, p.nonneg, bx, f + dm.NX);
         v[3] += (xv - o) * (xv - o);
       }
+      v[4] = tsv_pairs_at(z, f, dm.NX, dm.NY);
     }
   }
-  block_sum<4>(v, sh);
+  block_sum<5>(v, sh);
   if (threadIdx.x == 0) {
     part.at(kQDq1, b)[blockIdx.x] = v[0];
     part.at(kQDq2, b)[blockIdx.x] = v[1];
     part.at(kQL1, b)[blockIdx.x] = v[2];
     part.at(kQReg, b)[blockIdx.x] = v[3];
+    part.at(kQTsvZ, b)[blockIdx.x] = v[4];
   }
 }
 
@@ -179,9 +185,11 @@ __global__ void k_momentum(double* __restrict__ xall, double* __restrict__ zall,
   if (s.take_x) x[f] = xnv;
 }
 
-// elementwise copy of a per-problem vector (x = src) for every problem
-__global__ void k_copy_vec(double* __restrict__ dst, const double* __restrict__ src, ImgDims dm) {
+// per-problem vector copy dst = src for the problems passing `gate`
+__global__ void k_copy_gated(double* __restrict__ dst, const double* __restrict__ src, ImgDims dm,
+                             const ProbState* __restrict__ st, int gate) {
   int b = blockIdx.y;
+  if (!gate_ok(st[b], gate)) return;
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f < dm.N) dst[(size_t)b * dm.xstride + f] = src[(size_t)b * dm.xstride + f];
 }
@@ -200,6 +208,7 @@ struct CtrlCfg {
   // steps[0]: loop steps taken so far, steps[1]: budget after which every
   // still-active problem stops (device memory, set per solve)
   unsigned long long* steps;
+  int refresh_every;  // > 0: FP32 form, refresh the FP64 anchor this often
 };
 
 // status codes written to ProbState.status (values of enum mfista_status)
@@ -220,75 +229,71 @@ __device__ __forceinline__ double warp_partial_sum(const double* p, int n, int l
   return warp_sum(s);
 }
 
-__global__ void __launch_bounds__(256) k_control(const ProbParams* __restrict__ prm, ProbState* __restrict__ st, Partials part,
-                          CtrlCfg cfg, FinalOut* __restrict__ out, cudaGraphConditionalHandle handle,
-                          int set_handle, int* __restrict__ any_active) {
-  __shared__ int s_any, s_cap;
-  if (threadIdx.x == 0) {
-    s_any = 0;
-    s_cap = 0;
-    if (cfg.mode == kCtrlStep && cfg.steps) {
-      unsigned long long n = atomicAdd(cfg.steps, 1ull) + 1ull;
-      if (n >= cfg.steps[1]) s_cap = 1;
+// One CTA per problem.  The four warps reduce the partial sums (fixed order),
+// thread 0 runs the MFISTA scalar logic, and the last CTA to finish (atomic
+// ticket) ORs the active flags into the graph's WHILE condition.
+__global__ void __launch_bounds__(128) k_control(const ProbParams* __restrict__ prm, ProbState* __restrict__ st,
+                                                 Partials part, CtrlCfg cfg, FinalOut* __restrict__ out,
+                                                 cudaGraphConditionalHandle handle, int set_handle,
+                                                 int* __restrict__ any_active, unsigned int* __restrict__ ticket) {
+  __shared__ double red[kNumQ];
+  __shared__ int s_skip;
+  const int b = blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_skip = (cfg.mode == kCtrlStep && !st[b].active) ? 1 : 0;
+  __syncthreads();
+  if (!s_skip) {
+    for (int q = warp; q < kNumQ; q += 4) {
+      bool need = q == kQChiX || q == kQL1 || q == kQReg;
+      if (cfg.mode == kCtrlStep) need = need || q == kQChiZ || q == kQTsvZ || q == kQDq1 || q == kQDq2;
+      if (cfg.mode == kCtrlFinal) need = need || q == kQNact;
+      double v = need ? warp_partial_sum(part.at(q, b), cfg.slots[q], lane) : 0.0;
+      if (lane == 0) red[q] = v;
     }
   }
   __syncthreads();
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int b = warp; b < cfg.B; b += nw) {
-    ProbState s = st[b];  // every lane reads; lane 0 writes back
+  if (threadIdx.x == 0) {
+    ProbState s = st[b];
     const ProbParams p = prm[b];
-    if (cfg.mode == kCtrlStep && !s.active) {
-      // finished on an earlier step: its last momentum update already ran
-      if (lane == 0 && s.accepted) st[b].accepted = 0;
-      continue;
-    }
-    double chiX = warp_partial_sum(part.at(kQChiX, b), cfg.slots[kQChiX], lane);
-    double l1 = warp_partial_sum(part.at(kQL1, b), cfg.slots[kQL1], lane);
-    double reg = warp_partial_sum(part.at(kQReg, b), cfg.slots[kQReg], lane);
-    double chiZ = 0, tsvZ = 0, dq1 = 0, dq2 = 0, nact = 0;
-    if (cfg.mode == kCtrlStep) {
-      chiZ = warp_partial_sum(part.at(kQChiZ, b), cfg.slots[kQChiZ], lane);
-      tsvZ = warp_partial_sum(part.at(kQTsvZ, b), cfg.slots[kQTsvZ], lane);
-      dq1 = warp_partial_sum(part.at(kQDq1, b), cfg.slots[kQDq1], lane);
-      dq2 = warp_partial_sum(part.at(kQDq2, b), cfg.slots[kQDq2], lane);
-    }
-    if (cfg.mode == kCtrlFinal) nact = warp_partial_sum(part.at(kQNact, b), cfg.slots[kQNact], lane);
-    if (lane == 0) {
-      const bool tsv_on = cfg.form == kFormTSV && p.lambda_tsv > 0;
-      if (cfg.mode == kCtrlInit) {
-        double cost = cfg.fscale * chiX + p.lambda_l1 * l1;
-        if (cfg.form == kFormTV) cost += p.lambda_tv * reg;
-        else if (tsv_on) cost += p.lambda_tsv * reg;
-        s.cost_now = cost;
-        s.l1x = l1;
-        s.c = p.cinit;
-        s.mu = 1.0;
-        s.iter = 0;
+    const bool tsv_on = cfg.form == kFormTSV && p.lambda_tsv > 0;
+    const double chiX = red[kQChiX], l1 = red[kQL1], reg = red[kQReg];
+    if (s_skip) {
+      s.accepted = 0;  // finished on an earlier step: its last momentum update already ran
+    } else if (cfg.mode == kCtrlInit) {
+      double cost = cfg.fscale * chiX + p.lambda_l1 * l1;
+      if (cfg.form == kFormTV) cost += p.lambda_tv * reg;
+      else if (tsv_on) cost += p.lambda_tsv * reg;
+      s.cost_now = cost;
+      s.l1x = l1;
+      s.c = p.cinit;
+      s.mu = 1.0;
+      s.iter = 0;
+      s.trial = 0;
+      s.iters_out = 0;
+      s.accepted = 0;
+      s.take_x = 0;
+      s.active = (p.maxiter > 0 && s.status == 0) ? 1 : 0;
+      s.need_grad = s.active;
+      s.refresh = 0;
+    } else if (cfg.mode == kCtrlStep) {
+      const bool capped = cfg.steps && (cfg.steps[0] + 1ull >= cfg.steps[1]);
+      if (s.need_grad) {  // a new outer iteration began with this step
+        s.cost[s.iter % kCostRing] = s.cost_now;
+        s.qcore = cfg.fscale * red[kQChiZ] + (tsv_on ? p.lambda_tsv * red[kQTsvZ] : 0.0);
         s.trial = 0;
-        s.iters_out = 0;
-        s.accepted = 0;
-        s.take_x = 0;
-        s.active = (p.maxiter > 0 && s.status == 0) ? 1 : 0;
-        s.need_grad = s.active;
-      } else if (cfg.mode == kCtrlStep) {
-        if (s.need_grad) {  // a new outer iteration began with this step
-          s.cost[s.iter % kCostRing] = s.cost_now;
-          s.qcore = cfg.fscale * chiZ + (tsv_on ? p.lambda_tsv * tsvZ : 0.0);
-          s.trial = 0;
-          s.need_grad = 0;
-        }
-        s.accepted = 0;
-        double fval = cfg.fscale * chiX + (tsv_on ? p.lambda_tsv * reg : 0.0);
-        double qval = (-dq1 + s.c * dq2 / 2) + s.qcore;
-        if (isnan(fval) || isnan(qval) || s_cap) {
-          // NaN never passes the backtracking test; the reference would retry
-          // maxiter times per iteration.  Stop this problem with a status.
-          s.status = s_cap ? kStatusStepCap : kStatusNonFinite;
-          s.active = 0;
-          s.iters_out = s.iter + 1;
-          st[b] = s;
-          continue;
-        }
+        s.need_grad = 0;
+        s.refresh = 0;
+      }
+      s.accepted = 0;
+      double fval = cfg.fscale * chiX + (tsv_on ? p.lambda_tsv * reg : 0.0);
+      double qval = (-red[kQDq1] + s.c * red[kQDq2] / 2) + s.qcore;
+      if (isnan(fval) || isnan(qval) || capped) {
+        // NaN never passes the backtracking test; the reference would retry
+        // maxiter times per iteration.  Stop this problem with a status.
+        s.status = capped ? kStatusStepCap : kStatusNonFinite;
+        s.active = 0;
+        s.iters_out = s.iter + 1;
+      } else {
         bool finish = fval <= qval;
         if (!finish) {
           s.c *= kEta;
@@ -330,34 +335,40 @@ __global__ void __launch_bounds__(256) k_control(const ProbParams* __restrict__ 
               s.iters_out = p.maxiter;
             } else {
               s.need_grad = 1;
+              s.refresh = (cfg.refresh_every > 0 && s.iter % cfg.refresh_every == 0) ? 1 : 0;
             }
           }
         }
-      } else {  // final summary (calc_result_*)
-        FinalOut o;
-        int rk = reg_kind(p, cfg.form, 1);
-        o.sq_error = 2 * (cfg.fscale * chiX);
-        o.l1cost = l1;
-        o.regcost = reg;
-        o.n_active = nact;
-        double fc = o.sq_error / 2;
-        if (p.lambda_l1 > 0) fc += p.lambda_l1 * l1;
-        if (rk == 1) fc += p.lambda_tsv * reg;
-        else if (rk == 2) fc += p.lambda_tv * reg;
-        o.finalcost = fc;
-        o.lip = s.c;
-        o.iters = s.iters_out;
-        o.status = s.status;
-        out[b] = o;
       }
-      st[b] = s;
-      if (s.active) atomicOr(&s_any, 1);
+    } else {  // final summary (calc_result_*)
+      FinalOut o;
+      int rk = reg_kind(p, cfg.form, 1);
+      o.sq_error = 2 * (cfg.fscale * chiX);
+      o.l1cost = l1;
+      o.regcost = reg;
+      o.n_active = red[kQNact];
+      double fc = o.sq_error / 2;
+      if (p.lambda_l1 > 0) fc += p.lambda_l1 * l1;
+      if (rk == 1) fc += p.lambda_tsv * reg;
+      else if (rk == 2) fc += p.lambda_tv * reg;
+      o.finalcost = fc;
+      o.lip = s.c;
+      o.iters = s.iters_out;
+      o.status = s.status;
+      out[b] = o;
     }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    if (set_handle) cudaGraphSetConditional(handle, s_any ? 1u : 0u);
-    if (any_active) *any_active = s_any;
+    st[b] = s;
+    __threadfence();
+    unsigned int t = atomicAdd(ticket, 1u);
+    if (t == gridDim.x - 1) {  // last problem done: publish the loop condition
+      __threadfence();
+      int any = 0;
+      for (int k = 0; k < gridDim.x; ++k) any |= ((volatile ProbState*)st)[k].active;
+      if (set_handle) cudaGraphSetConditional(handle, any ? 1u : 0u);
+      if (any_active) *any_active = any;
+      if (cfg.mode == kCtrlStep && cfg.steps) cfg.steps[0] += 1ull;
+      *ticket = 0u;
+    }
   }
 }
 

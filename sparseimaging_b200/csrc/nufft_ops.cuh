@@ -109,7 +109,7 @@ template <typename T>
 __global__ void k_nufft_rows_fwd(const double* __restrict__ xall, long xstride, const double* __restrict__ e4,
                                  cplx<T>* __restrict__ gall, long gstride, int nx, int ny, FftDev<T> fh,
                                  const cplx<T>* __restrict__ tw2h, const ProbState* __restrict__ st, int gate,
-                                 int rows_per_cta) {
+                                 int rows_per_cta, const double* __restrict__ suball) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   int b = blockIdx.y;
   if (!gate_ok(st[b], gate)) return;
@@ -118,6 +118,9 @@ __global__ void k_nufft_rows_fwd(const double* __restrict__ xall, long xstride, 
   cplx<T>* A = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* Bf = A + (size_t)rows_per_cta * ld;
   const double* x = xall + (size_t)b * xstride;
+  // defect correction: transform x - x_anchor (the anchor's model is added
+  // back in FP64 at the interpolation)
+  const double* sub = suball ? suball + (size_t)b * xstride : nullptr;
   cplx<T>* g = gall + (size_t)b * gstride;
   int i0 = blockIdx.x * rows_per_cta;
   int nrows = min(rows_per_cta, nx - i0);
@@ -126,8 +129,14 @@ __global__ void k_nufft_rows_fwd(const double* __restrict__ xall, long xstride, 
     int i = i0 + rr;
     int j0 = uncentre_index(2 * m, ny), j1 = uncentre_index(2 * m + 1, ny);
     T a = 0, c = 0;
-    if (j0 >= 0) a = (T)(x[(size_t)i * ny + j0] * e4[(size_t)i * ny + j0]);
-    if (j1 >= 0) c = (T)(x[(size_t)i * ny + j1] * e4[(size_t)i * ny + j1]);
+    if (j0 >= 0) {
+      size_t f = (size_t)i * ny + j0;
+      a = (T)((sub ? x[f] - sub[f] : x[f]) * e4[f]);
+    }
+    if (j1 >= 0) {
+      size_t f = (size_t)i * ny + j1;
+      c = (T)((sub ? x[f] - sub[f] : x[f]) * e4[f]);
+    }
     A[rr * ld + m] = mk<T>(a, c);
   }
   __syncthreads();
@@ -192,7 +201,8 @@ __global__ void k_nufft_cols(cplx<T>* __restrict__ gall, long gstride, int nx, i
 template <typename T>
 __global__ void k_nufft_interp(NufftGeom<T> geo, const cplx<T>* __restrict__ gall, long gstride, int nx, int ny,
                                double inv_mm, const ProbState* __restrict__ st, int gate, Partials part, int qchi,
-                               cplx<T>* __restrict__ y2) {
+                               cplx<T>* __restrict__ y2, const double2* __restrict__ ax_base,
+                               double2* __restrict__ ax_out) {
   __shared__ double sh[32];
   int b = blockIdx.y;
   if (!gate_ok(st[b], gate)) return;
@@ -236,15 +246,21 @@ __global__ void k_nufft_interp(NufftGeom<T> geo, const cplx<T>* __restrict__ gal
     }
     if (lane == 0) {
       double fr = (double)accr * inv_mm, fi = (double)acci * inv_mm;
+      const size_t e = b * geo.y2_bstride + k;
+      if (ax_base) {
+        fr += ax_base[e].x;
+        fi += ax_base[e].y;
+      }
+      if (ax_out) ax_out[e] = make_double2(fr, fi);
       double w = geo.weight[k];
       double rr = (geo.vis_r[k] - fr) * w;
       double ri = (geo.vis_i[k] - fi) * w;
       chi[0] = rr * rr + ri * ri;
-      if (y2) y2[b * geo.y2_bstride + k] = mk<T>((T)(rr * w), (T)(ri * w));
+      if (y2) y2[e] = mk<T>((T)(rr * w), (T)(ri * w));
     }
   }
   block_sum<1>(chi, sh);
-  if (threadIdx.x == 0) part.at(qchi, b)[blockIdx.x] = chi[0];
+  if (threadIdx.x == 0 && qchi >= 0) part.at(qchi, b)[blockIdx.x] = chi[0];
 }
 
 // ---------------------------------------------------------------------------
@@ -309,20 +325,20 @@ __global__ void k_nufft_spread(NufftGeom<T> geo, const cplx<T>* __restrict__ y2,
         // the reference adds the two contributions of one point in ly order
         // (direct first on a tie), which is kept here
         if (d && (!mi || lyd <= lym)) {
-          T wy = s_wy[pp][lyd], wx = s_wx[pp][lxd];
-          ar += (vr * wy) * wx * T(0.5);
-          ai += (vi * wy) * wx * T(0.5);
+          const T hw = s_wy[pp][lyd] * s_wx[pp][lxd] * T(0.5);
+          ar += vr * hw;
+          ai += vi * hw;
           d = false;
         }
         if (mi) {
-          T wy = s_wy[pp][lym], wx = s_wx[pp][lxm];
-          ar += (vr * wy) * wx * T(0.5);
-          ai -= (vi * wy) * wx * T(0.5);
+          const T hw = s_wy[pp][lym] * s_wx[pp][lxm] * T(0.5);
+          ar += vr * hw;
+          ai += -vi * hw;
         }
         if (d) {
-          T wy = s_wy[pp][lyd], wx = s_wx[pp][lxd];
-          ar += (vr * wy) * wx * T(0.5);
-          ai += (vi * wy) * wx * T(0.5);
+          const T hw = s_wy[pp][lyd] * s_wx[pp][lxd] * T(0.5);
+          ar += vr * hw;
+          ai += vi * hw;
         }
       }
     }
@@ -420,6 +436,251 @@ __global__ void k_nufft_rows_inv(const cplx<T>* __restrict__ gall, long gstride,
   if (qtsv >= 0) {
     block_sum<1>(acc, sh);
     if (threadIdx.x == 0) part.at(qtsv, b)[blockIdx.x] = acc[0];
+  }
+}
+
+}  // namespace mf
+
+// ===========================================================================
+// Shared-geometry batch (every problem of the batch uses the same uv points,
+// e.g. a lambda grid).  The tap geometry of a point is computed once and
+// applied to a chunk of problems; grids stay problem-major.
+// ===========================================================================
+namespace mf {
+
+template <typename T> struct SharedChunk;
+template <> struct SharedChunk<float> {
+  static constexpr int kInterp = 16;  // problems per interpolation CTA
+  static constexpr int kSpread = 16;  // problems per spreading CTA
+  static constexpr int kInterpMinBlocks = 2;
+};
+template <> struct SharedChunk<double> {
+  static constexpr int kInterp = 8;
+  static constexpr int kSpread = 8;
+  static constexpr int kInterpMinBlocks = 2;
+};
+
+// interpolation: one warp per point, lanes over the 576 taps (18 each) with
+// cell and weight held in registers, looping over the CTA's problem chunk
+constexpr int kInterpPtsPerWarp = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(256, SharedChunk<T>::kInterpMinBlocks) k_nufft_interp_shared(NufftGeom<T> geo, const cplx<T>* __restrict__ gall,
+                                                             long gstride, int nx, int ny, double inv_mm,
+                                                             const ProbState* __restrict__ st, int gate,
+                                                             Partials part, int qchi, cplx<T>* __restrict__ y2,
+                                                             int B, const double2* __restrict__ ax_base,
+                                                             double2* __restrict__ ax_out) {
+  constexpr int PB = SharedChunk<T>::kInterp;
+  constexpr int NT = (kTaps * kTaps) / 32;
+  __shared__ double s_chi[8][PB];
+  __shared__ int s_act[PB];
+  const int b0 = blockIdx.y * PB;
+  if (threadIdx.x < PB) {
+    int b = b0 + threadIdx.x;
+    s_act[threadIdx.x] = (b < B && gate_ok(st[b], gate)) ? 1 : 0;
+  }
+  __syncthreads();
+  int any = 0;
+#pragma unroll
+  for (int i = 0; i < PB; ++i) any |= s_act[i];
+  if (!any) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int mtot = geo.pt_hi[0];
+  if (lane < PB) s_chi[warp][lane] = 0.0;
+  __syncwarp();
+  for (int q = 0; q < kInterpPtsPerWarp; ++q) {
+    const int k = (blockIdx.x * 8 + warp) * kInterpPtsPerWarp + q;
+    if (k >= mtot) break;
+    int cell[NT];
+    T wgt[NT];
+    const int mxk = geo.mx[k], myk = geo.my[k];
+    const T* wxk = geo.wx + (size_t)k * kTaps;
+    const T* wyk = geo.wy + (size_t)k * kTaps;
+#pragma unroll
+    for (int s = 0; s < NT; ++s) {
+      int t = lane + 32 * s;
+      int lx = t / kTaps, ly = t - lx * kTaps;
+      int m = myk + ly - (kMSP - 1);
+      int mxm = mxk + lx - (kMSP - 1);
+      int col = half_col(m, ny), row, mirror = 0;
+      if (col >= 0) {
+        row = wrap_row(mxm, nx);
+      } else {
+        col = half_col(-m, ny);
+        row = wrap_row(-mxm, nx);
+        mirror = 1;
+      }
+      if (col >= 0 && row >= 0) {
+        cell[s] = (row * (ny + 1) + col) | (mirror << 30);
+        wgt[s] = wyk[ly] * wxk[lx];
+      } else {
+        cell[s] = -1;
+        wgt[s] = 0;
+      }
+    }
+    const double w = geo.weight[k];
+    const double vr = geo.vis_r[k], vi = geo.vis_i[k];
+#pragma unroll 1
+    for (int i = 0; i < PB; ++i) {
+      if (!s_act[i]) continue;
+      const int b = b0 + i;
+      const cplx<T>* g = gall + (size_t)b * gstride;
+      T accr = 0, acci = 0;
+#pragma unroll
+      for (int s = 0; s < NT; ++s) {
+        int cc = cell[s];
+        if (cc >= 0) {
+          cplx<T> gv = g[cc & 0x3fffffff];
+          accr += gv.x * wgt[s];
+          // NU_SIGN on the imaginary part of direct taps, + on mirrored ones
+          acci += ((cc >> 30) ? gv.y : -gv.y) * wgt[s];
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        accr += __shfl_xor_sync(0xffffffffu, accr, o);
+        acci += __shfl_xor_sync(0xffffffffu, acci, o);
+      }
+      if (lane == 0) {
+        double fr = (double)accr * inv_mm, fi = (double)acci * inv_mm;
+        const size_t e = (size_t)b * geo.y2_bstride + k;
+        if (ax_base) {
+          fr += ax_base[e].x;
+          fi += ax_base[e].y;
+        }
+        if (ax_out) ax_out[e] = make_double2(fr, fi);
+        double rr = (vr - fr) * w;
+        double ri = (vi - fi) * w;
+        s_chi[warp][i] += rr * rr + ri * ri;
+        if (y2) y2[e] = mk<T>((T)(rr * w), (T)(ri * w));
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < PB && s_act[threadIdx.x] && qchi >= 0) {
+    double c = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) c += s_chi[w][threadIdx.x];
+    part.at(qchi, b0 + threadIdx.x)[blockIdx.x] = c;
+  }
+}
+
+// spreading: one CTA per (16 x 16 tile, problem chunk), one thread per cell
+// holding the chunk's accumulators; the tile's points (taps, the chunk's
+// residuals and 16-bit masks of the tile rows / columns their direct or
+// mirrored footprint covers) are staged through shared memory and read as
+// broadcasts, so a point that misses a cell costs one mask test.
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_nufft_spread_shared(NufftGeom<T> geo, const cplx<T>* __restrict__ y2,
+                                                             cplx<T>* __restrict__ gall, long gstride, int nx,
+                                                             int ny, int ntiles, const ProbState* __restrict__ st,
+                                                             int gate, int B) {
+  constexpr int PB = SharedChunk<T>::kSpread;
+  constexpr int P = 32;
+  constexpr int TILE = 16;
+  __shared__ int s_ox[P], s_oy[P];          // 11 - mx, 11 - my
+  __shared__ unsigned int s_mask[P];        // rows (low 16 bits) | cols (high 16 bits)
+  __shared__ T s_wx[P][kTaps], s_wy[P][kTaps];
+  __shared__ __align__(16) cplx<T> s_r[P][PB];
+  __shared__ int s_act[PB];
+  const int b0 = blockIdx.y * PB;
+  if (threadIdx.x < PB) {
+    int b = b0 + threadIdx.x;
+    s_act[threadIdx.x] = (b < B && gate_ok(st[b], gate)) ? 1 : 0;
+  }
+  __syncthreads();
+  int any = 0;
+#pragma unroll
+  for (int i = 0; i < PB; ++i) any |= s_act[i];
+  if (!any) return;
+  const int tile = blockIdx.x;
+  const int ntc = (ny + 1 + TILE - 1) / TILE;
+  const int tr = tile / ntc, tc = tile - tr * ntc;
+  const int ty = threadIdx.x / TILE, tx = threadIdx.x - ty * TILE;
+  const int row0 = tr * TILE, col0 = tc * TILE;
+  const int row = row0 + ty, col = col0 + tx;
+  const bool valid = row < 2 * nx && col <= ny;
+  const int mrow = row < nx ? row : row - 2 * nx;
+  const int mcol = col < ny ? col : -ny;
+  T ar[PB], ai[PB];
+#pragma unroll
+  for (int i = 0; i < PB; ++i) ar[i] = ai[i] = 0;
+  const int beg = geo.tile_ptr[tile], end = geo.tile_ptr[tile + 1];
+  for (int c0 = beg; c0 < end; c0 += P) {
+    const int np = min(P, end - c0);
+    __syncthreads();
+    if (threadIdx.x < np) {
+      const int t = threadIdx.x;
+      const int k = geo.tile_pts[c0 + t];
+      const int mx = geo.mx[k], my = geo.my[k];
+      s_ox[t] = (kMSP - 1) - mx;
+      s_oy[t] = (kMSP - 1) - my;
+      // tile rows / columns reached by the direct or mirrored footprint
+      unsigned int rm = 0, cm = 0;
+      for (int q = 0; q < TILE; ++q) {
+        int r = row0 + q, cc = col0 + q;
+        int mr = r < nx ? r : r - 2 * nx;
+        int mc = cc < ny ? cc : -ny;
+        if (r < 2 * nx && ((unsigned)(mr - mx + (kMSP - 1)) < (unsigned)kTaps ||
+                           (unsigned)(-mr - mx + (kMSP - 1)) < (unsigned)kTaps))
+          rm |= 1u << q;
+        if (cc <= ny && ((unsigned)(mc - my + (kMSP - 1)) < (unsigned)kTaps ||
+                         (unsigned)(-mc - my + (kMSP - 1)) < (unsigned)kTaps))
+          cm |= 1u << q;
+      }
+      s_mask[t] = rm | (cm << 16);
+    }
+    for (int t = threadIdx.x; t < np * kTaps; t += blockDim.x) {
+      int pp = t / kTaps, j = t - pp * kTaps;
+      int k = geo.tile_pts[c0 + pp];
+      s_wx[pp][j] = geo.wx[(size_t)k * kTaps + j];
+      s_wy[pp][j] = geo.wy[(size_t)k * kTaps + j];
+    }
+    for (int t = threadIdx.x; t < np * PB; t += blockDim.x) {
+      int pp = t / PB, i = t - pp * PB;
+      int k = geo.tile_pts[c0 + pp];
+      cplx<T> r = mk<T>(0, 0);
+      if (s_act[i]) {
+        r = y2[(size_t)(b0 + i) * geo.y2_bstride + k];
+        r.y = -r.y;  // NU_SIGN * Fin_i
+      }
+      s_r[pp][i] = r;
+    }
+    __syncthreads();
+    if (valid) {
+      const unsigned int mybits = (1u << ty) | (1u << (16 + tx));
+      for (int pp = 0; pp < np; ++pp) {
+        if ((s_mask[pp] & mybits) != mybits) continue;
+        const int ox = s_ox[pp], oy = s_oy[pp];
+        const int lxd = mrow + ox, lyd = mcol + oy;
+        const int lxm = ox - mrow, lym = oy - mcol;
+        const bool d = (unsigned)lxd < (unsigned)kTaps && (unsigned)lyd < (unsigned)kTaps;
+        const bool mi = (unsigned)lxm < (unsigned)kTaps && (unsigned)lym < (unsigned)kTaps;
+        if (!(d || mi)) continue;
+        // the reference adds the two contributions of one point in ly order
+        const bool mfirst = mi && d && lym < lyd;
+        for (int pass = 0; pass < 2; ++pass) {
+          const bool use_m = (pass == 0) ? mfirst : (mi && !mfirst);
+          const bool use_d = (pass == 0) ? (d && !mfirst) : (d && mfirst);
+          if (!(use_m || use_d)) continue;
+          const T w = use_m ? s_wy[pp][lym] * s_wx[pp][lxm] : s_wy[pp][lyd] * s_wx[pp][lxd];
+          const T hw = w * T(0.5);
+          const T hwi = use_m ? -hw : hw;
+#pragma unroll
+          for (int i = 0; i < PB; ++i) {
+            cplx<T> r = s_r[pp][i];
+            ar[i] += r.x * hw;
+            ai[i] += r.y * hwi;
+          }
+        }
+      }
+    }
+  }
+  if (valid) {
+#pragma unroll
+    for (int i = 0; i < PB; ++i)
+      if (s_act[i]) gall[(size_t)(b0 + i) * gstride + (size_t)row * (ny + 1) + col] = mk<T>(ar[i], ai[i]);
   }
 }
 

@@ -121,6 +121,7 @@ struct Ctx {
   double* z = nullptr;
   double* xnew = nullptr;
   double* dfdx = nullptr;
+  double* xa = nullptr;  // FP32 form: anchor images of the defect correction
   ProbParams* prm = nullptr;
   ProbState* st = nullptr;
   Partials part{};
@@ -142,6 +143,15 @@ struct Op {
   // 4 cols inv, 5 rows inv; returns its algorithmic bytes (compulsory reads
   // and writes of one launch over the whole batch), or < 0 if not defined
   virtual double launch_single(cudaStream_t s, int kernel) { (void)s; (void)kernel; return -1; }
+  // defect correction (FP32 operators): recompute the exact FP64 model of the
+  // anchors ctx.xa for the problems passing `gate`; forward_exact evaluates
+  // chi^2 with the FP64 operator (initial and final objective)
+  virtual bool corrected() const { return false; }
+  virtual void refresh_anchor(cudaStream_t s, int gate) { (void)s; (void)gate; }
+  virtual void forward_exact(cudaStream_t s, const double* src, int gate, int qchi, bool store) {
+    forward(s, src, gate, qchi, store);
+  }
+  virtual int launches_refresh() const { return 0; }
 };
 
 // ---------------------------------------------------------------------------
@@ -189,6 +199,8 @@ template <typename T> struct NufftOp : Op {
   Ctx& c;
   int nx, ny, B, mtot, mmax;
   bool shared;
+  std::unique_ptr<NufftOp<double>> exact;  // FP64 operator for the anchors
+  DevMem d_axa;                            // exact model of the anchors [y2 layout]
   DevMem d_u, d_v, d_mx, d_my, d_wx, d_wy, d_vr, d_vi, d_w, d_lo, d_hi, d_tptr, d_tpts, d_e4, d_grid, d_y2, tw2h;
   FftHost<T> fh, fcol;
   NufftGeom<T> geo{};
@@ -197,7 +209,7 @@ template <typename T> struct NufftOp : Op {
   long gstride = 0;
   double inv_mm = 0;
 
-  NufftOp(Ctx& ctx, const NufftInput& in) : c(ctx) {
+  NufftOp(Ctx& ctx, const NufftInput& in, bool correct = false) : c(ctx) {
     nx = in.Nx;
     ny = in.Ny;
     B = ctx.B;
@@ -243,7 +255,8 @@ template <typename T> struct NufftOp : Op {
     d_e4.alloc(sizeof(double) * nx * ny);
     k_nufft_prep_e4<<<cdiv(nx * ny, 256), 256>>>(d_e4.as<double>(), nx, ny);
     MF_LAUNCH_CK();
-    // spread tiles
+    // spread tiles (16 x 16 for the shared-geometry kernels)
+    if (shared) tile_r = tile_c = 16;
     ntiles = cdiv(2 * nx, tile_r) * cdiv(ny + 1, tile_c);
     int ngeo = shared ? 1 : B;
     std::vector<int> tptr;
@@ -279,6 +292,11 @@ template <typename T> struct NufftOp : Op {
     set_smem(k_nufft_rows_fwd<T>, smem_rows);
     set_smem(k_nufft_rows_inv<T>, smem_rows);
     set_smem(k_nufft_cols<T>, smem_cols);
+    if (correct && sizeof(T) == 4) {
+      exact.reset(new NufftOp<double>(ctx, in, false));
+      d_axa.alloc(sizeof(double2) * (size_t)y2n);
+      MF_CK(cudaMemset(d_axa.p, 0, d_axa.bytes));
+    }
     geo.mx = d_mx.as<int>();
     geo.my = d_my.as<int>();
     geo.wx = d_wx.as<T>();
@@ -296,26 +314,72 @@ template <typename T> struct NufftOp : Op {
     MF_CK(cudaDeviceSynchronize());
   }
 
-  int interp_blocks() const { return std::max(1, cdiv(mmax, 8)); }
+  int interp_blocks() const { return std::max(1, cdiv(mmax, shared ? 8 * kInterpPtsPerWarp : 8)); }
+  int interp_chunks() const { return cdiv(B, SharedChunk<T>::kInterp); }
+  int spread_chunks() const { return cdiv(B, SharedChunk<T>::kSpread); }
+
+  void launch_interp(cudaStream_t s, cplx<T>* g, int gate, int qchi, cplx<T>* y2, const double2* base = nullptr,
+                     double2* out = nullptr) {
+    if (shared)
+      k_nufft_interp_shared<T><<<dim3(interp_blocks(), interp_chunks()), 256, 0, s>>>(
+          geo, g, gstride, nx, ny, inv_mm, c.st, gate, c.part, qchi, y2, B, base, out);
+    else
+      k_nufft_interp<T><<<dim3(interp_blocks(), B), 256, 0, s>>>(geo, g, gstride, nx, ny, inv_mm, c.st, gate,
+                                                                 c.part, qchi, y2, base, out);
+    MF_LAUNCH_CK();
+  }
+
+  void launch_rows_fwd(cudaStream_t s, const double* src, int gate, const double* sub) {
+    k_nufft_rows_fwd<T><<<dim3(cdiv(nx, rpc), B), 256, smem_rows, s>>>(src, c.xstride, geo.e4, d_grid.as<cplx<T>>(),
+                                                                       gstride, nx, ny, fh.dev, tw2h.as<cplx<T>>(),
+                                                                       c.st, gate, rpc, sub);
+    MF_LAUNCH_CK();
+  }
+
+  bool corrected() const override { return exact != nullptr; }
+  int launches_refresh() const override { return exact ? 3 : 0; }
+
+  // exact FP64 model of the anchors: A x_a -> d_axa (owner's layout)
+  void refresh_anchor(cudaStream_t s, int gate) override {
+    if (!exact) return;
+    exact->launch_rows_fwd(s, c.xa, gate, nullptr);
+    exact->launch_cols_fwd(s, gate);
+    exact->launch_interp(s, exact->d_grid.template as<cplx<double>>(), gate, -1, nullptr, nullptr,
+                         d_axa.as<double2>());
+  }
+
+  void forward_exact(cudaStream_t s, const double* src, int gate, int qchi, bool store) override {
+    if (exact) exact->forward(s, src, gate, qchi, store);
+    else forward(s, src, gate, qchi, store);
+  }
+
+  void launch_cols_fwd(cudaStream_t s, int gate) {
+    k_nufft_cols<T><<<dim3(cdiv(ny + 1, cpc), B), 256, smem_cols, s>>>(d_grid.as<cplx<T>>(), gstride, nx, ny,
+                                                                       fcol.dev, -1, cpc, 1, 0, c.st, gate);
+    MF_LAUNCH_CK();
+  }
+
+  void launch_spread(cudaStream_t s, cplx<T>* g, int gate) {
+    if (shared)
+      k_nufft_spread_shared<T><<<dim3(ntiles, spread_chunks()), 256, 0, s>>>(geo, d_y2.as<cplx<T>>(), g, gstride, nx,
+                                                                             ny, ntiles, c.st, gate, B);
+    else
+      k_nufft_spread<T><<<dim3(ntiles, B), tile_r * tile_c, 0, s>>>(geo, d_y2.as<cplx<T>>(), g, gstride, nx, ny,
+                                                                    tile_r, tile_c, ntiles, c.st, gate);
+    MF_LAUNCH_CK();
+  }
 
   void forward(cudaStream_t s, const double* src, int gate, int qchi, bool store) override {
     cplx<T>* g = d_grid.as<cplx<T>>();
-    k_nufft_rows_fwd<T><<<dim3(cdiv(nx, rpc), B), 256, smem_rows, s>>>(src, c.xstride, geo.e4, g, gstride, nx, ny,
-                                                                       fh.dev, tw2h.as<cplx<T>>(), c.st, gate, rpc);
-    MF_LAUNCH_CK();
-    k_nufft_cols<T><<<dim3(cdiv(ny + 1, cpc), B), 256, smem_cols, s>>>(g, gstride, nx, ny, fcol.dev, -1, cpc, 1, 0,
-                                                                       c.st, gate);
-    MF_LAUNCH_CK();
-    k_nufft_interp<T><<<dim3(interp_blocks(), B), 256, 0, s>>>(geo, g, gstride, nx, ny, inv_mm, c.st, gate, c.part,
-                                                               qchi, store ? d_y2.as<cplx<T>>() : nullptr);
-    MF_LAUNCH_CK();
+    // with defect correction: A v = A x_a (FP64) + A32 (v - x_a)
+    launch_rows_fwd(s, src, gate, exact ? c.xa : nullptr);
+    launch_cols_fwd(s, gate);
+    launch_interp(s, g, gate, qchi, store ? d_y2.as<cplx<T>>() : nullptr, exact ? d_axa.as<double2>() : nullptr);
   }
 
   void adjoint(cudaStream_t s, const double* z_tsv, int qtsv) override {
     cplx<T>* g = d_grid.as<cplx<T>>();
-    k_nufft_spread<T><<<dim3(ntiles, B), tile_r * tile_c, 0, s>>>(geo, d_y2.as<cplx<T>>(), g, gstride, nx, ny,
-                                                                  tile_r, tile_c, ntiles, c.st, kGateGrad);
-    MF_LAUNCH_CK();
+    launch_spread(s, g, kGateGrad);
     k_nufft_cols<T><<<dim3(cdiv(ny + 1, cpc), B), 256, smem_cols, s>>>(g, gstride, nx, ny, fcol.dev, +1, cpc, 0, 1,
                                                                        c.st, kGateGrad);
     MF_LAUNCH_CK();
@@ -340,19 +404,13 @@ template <typename T> struct NufftOp : Op {
     const double pts_res = shared ? (double)B * mtot : (double)mtot;  // per-problem residuals
     switch (kernel) {
       case 0:
-        k_nufft_interp<T><<<dim3(interp_blocks(), B), 256, 0, s>>>(geo, g, gstride, nx, ny, inv_mm, c.st, kGateAll,
-                                                                   c.part, kQChiX, d_y2.as<cplx<T>>());
-        MF_LAUNCH_CK();
+        launch_interp(s, g, kGateAll, kQChiX, d_y2.as<cplx<T>>());
         return B * G * cs + pts_geo * (8 + 2 * kTaps * ts + 24) + pts_res * cs;
       case 1:
-        k_nufft_spread<T><<<dim3(ntiles, B), tile_r * tile_c, 0, s>>>(geo, d_y2.as<cplx<T>>(), g, gstride, nx, ny,
-                                                                      tile_r, tile_c, ntiles, c.st, kGateGrad);
-        MF_LAUNCH_CK();
+        launch_spread(s, g, kGateGrad);
         return pts_geo * (8 + 2 * kTaps * ts) + pts_res * cs + B * G * cs;
       case 2:
-        k_nufft_rows_fwd<T><<<dim3(cdiv(nx, rpc), B), 256, smem_rows, s>>>(
-            c.z, c.xstride, geo.e4, g, gstride, nx, ny, fh.dev, tw2h.as<cplx<T>>(), c.st, kGateAll, rpc);
-        MF_LAUNCH_CK();
+        launch_rows_fwd(s, c.z, kGateAll, nullptr);
         return B * N * 8 + N * 8 + B * half_rows * cs;
       case 3:
         k_nufft_cols<T><<<dim3(cdiv(ny + 1, cpc), B), 256, smem_cols, s>>>(g, gstride, nx, ny, fcol.dev, -1, cpc, 1, 0,
@@ -477,8 +535,10 @@ template <typename T> struct FftVarOp : Op {
 struct DftOp : Op {
   Ctx& c;
   DftGeom g{};
-  DevMem d_A, d_y, d_part, d_resid;
+  DevMem d_A, d_y, d_part, d_resid, d_atr;
   int B;
+  bool gemm = false;     // batched problems: GEMMs instead of per-problem GEMVs
+  int mchunk = 0, nmchunk = 0;
 
   DftOp(Ctx& ctx, const double* A, const double* y, int M, int N) : c(ctx) {
     B = ctx.B;
@@ -490,6 +550,14 @@ struct DftOp : Op {
     g.N = N;
     g.chunk = 64;
     g.nchunk = cdiv(N, g.chunk);
+    gemm = B > 1;
+    if (gemm) {  // split-K so that the tiles fill the GPU
+      g.chunk = std::max(kGK, cdiv(cdiv(N, 4), kGK) * kGK);
+      g.nchunk = cdiv(N, g.chunk);
+      mchunk = std::max(kGK, cdiv(cdiv(M, 8), kGK) * kGK);
+      nmchunk = cdiv(M, mchunk);
+      d_atr.alloc(sizeof(double) * (size_t)B * nmchunk * std::max(N, 1));
+    }
     d_part.alloc(sizeof(double) * (size_t)B * g.nchunk * std::max(M, 1));
     d_resid.alloc(sizeof(double) * (size_t)B * std::max(M, 1));
     g.az_part = d_part.as<double>();
@@ -497,14 +565,26 @@ struct DftOp : Op {
   }
 
   void forward(cudaStream_t s, const double* src, int gate, int qchi, bool store) override {
-    k_dft_az<<<dim3(std::max(1, cdiv(g.M, 256)), g.nchunk, B), 256, g.chunk * sizeof(double), s>>>(g, src, c.xstride,
-                                                                                                     c.st, gate);
+    if (gemm)
+      k_dft_az_gemm<<<dim3(cdiv(g.M, kGT), g.nchunk, cdiv(B, kGT)), 256, 0, s>>>(g, src, c.xstride, c.st, gate, B);
+    else
+      k_dft_az<<<dim3(std::max(1, cdiv(g.M, 256)), g.nchunk, B), 256, g.chunk * sizeof(double), s>>>(
+          g, src, c.xstride, c.st, gate);
     MF_LAUNCH_CK();
     k_dft_resid<<<dim3(std::max(1, cdiv(g.M, 256)), B), 256, 0, s>>>(g, c.st, gate, c.part, qchi, store ? 1 : 0);
     MF_LAUNCH_CK();
   }
 
   void adjoint(cudaStream_t s, const double* z_tsv, int qtsv) override {
+    if (gemm) {
+      k_dft_atr_gemm<<<dim3(cdiv(g.N, kGT), nmchunk, cdiv(B, kGT)), 256, 0, s>>>(g, d_atr.as<double>(), mchunk,
+                                                                                 nmchunk, c.st, kGateGrad, B);
+      MF_LAUNCH_CK();
+      k_dft_atr_finish<<<dim3(cdiv(g.N, 256), B), 256, 0, s>>>(g, d_atr.as<double>(), nmchunk, c.dfdx, c.xstride,
+                                                               z_tsv, c.prm, c.tsvNX, c.tsvNY, c.st, kGateGrad);
+      MF_LAUNCH_CK();
+      return;
+    }
     k_dft_atr<<<dim3(cdiv(g.N, 8), B), 256, 0, s>>>(g, c.dfdx, c.xstride, z_tsv, c.prm, c.tsvNX, c.tsvNY, c.st,
                                                      kGateGrad, c.part, qtsv);
     MF_LAUNCH_CK();
@@ -514,7 +594,7 @@ struct DftOp : Op {
   int tsv_slots() const override { return cdiv(g.N, 8); }
   double fscale() const override { return 0.5; }
   int launches_forward() const override { return 2; }
-  int launches_adjoint() const override { return 1; }
+  int launches_adjoint() const override { return gemm ? 2 : 1; }
 };
 
 // ---------------------------------------------------------------------------
@@ -526,8 +606,9 @@ struct Solver {
   int form = kFormTSV;
   int precision = MFISTA_FP64;
   int fgp_iter = 100;
+  int refresh_every = 0;  // defect correction: anchor refresh period (outer iterations)
   int step_cap = 0;
-  DevMem d_x, d_z, d_xnew, d_dfdx, d_prm, d_st, d_part, d_out, d_box, d_fgp, d_steps;
+  DevMem d_x, d_z, d_xnew, d_dfdx, d_xa, d_prm, d_st, d_part, d_out, d_box, d_fgp, d_steps, d_ticket;
   unsigned long long step_budget = 0;
   ImgDims dm{};
   cudaStream_t stream = nullptr, cap_stream = nullptr;
@@ -576,12 +657,16 @@ struct Solver {
     d_st.alloc(sizeof(ProbState) * B);
     d_out.alloc(sizeof(FinalOut) * B);
     d_steps.alloc(2 * sizeof(unsigned long long));
+    d_ticket.alloc(sizeof(unsigned int));
+    MF_CK(cudaMemset(d_ticket.p, 0, sizeof(unsigned int)));
     ctx.x = d_x.as<double>();
     ctx.z = d_z.as<double>();
     ctx.xnew = d_xnew.as<double>();
     ctx.dfdx = d_dfdx.as<double>();
     ctx.prm = d_prm.as<ProbParams>();
     ctx.st = d_st.as<ProbState>();
+    d_xa.alloc(sizeof(double) * (size_t)B * N);
+    ctx.xa = d_xa.as<double>();
     dm.N = N;
     dm.NX = NX;
     dm.NY = NY;
@@ -604,7 +689,9 @@ struct Solver {
     ctx.part.slots = slots;
     ctx.part.B = ctx.B;
     if (form == kFormTV) setup_fgp();
-    per_step_launches = op->launches_forward() * 2 + op->launches_adjoint() + 3 + (form == kFormTV ? 1 : 0);
+    refresh_every = op->corrected() ? 32 : 0;
+    per_step_launches = op->launches_forward() * 2 + op->launches_adjoint() + 3 + (form == kFormTV ? 1 : 0) +
+                        (op->corrected() ? 1 + op->launches_refresh() : 0);
     fixed_launches = 2 * (op->launches_forward() + 2) + 1;
     const char* hl = getenv("MFISTA_HOST_LOOP");
     host_loop = hl && hl[0] == '1';
@@ -709,7 +796,7 @@ struct Solver {
     memset(&cfg, 0, sizeof(cfg));
     cfg.slots[kQChiZ] = op->chi_slots();
     cfg.slots[kQChiX] = op->chi_slots();
-    cfg.slots[kQTsvZ] = form == kFormTSV ? op->tsv_slots() : 0;
+    cfg.slots[kQTsvZ] = form == kFormTSV ? img_blocks() : 0;
     cfg.slots[kQDq1] = img_blocks();
     cfg.slots[kQDq2] = img_blocks();
     cfg.slots[kQL1] = img_blocks();
@@ -720,20 +807,28 @@ struct Solver {
     cfg.mode = mode;
     cfg.B = ctx.B;
     cfg.steps = d_steps.as<unsigned long long>();
+    cfg.refresh_every = refresh_every;
     return cfg;
   }
 
   void launch_control(cudaStream_t s, int mode, cudaGraphConditionalHandle h, int set_handle) {
-    k_control<<<1, 256, 0, s>>>(ctx.prm, ctx.st, ctx.part, ctrl_cfg(mode), d_out.as<FinalOut>(), h, set_handle,
-                                  d_any);
+    k_control<<<ctx.B, 128, 0, s>>>(ctx.prm, ctx.st, ctx.part, ctrl_cfg(mode), d_out.as<FinalOut>(), h, set_handle,
+                                     d_any, d_ticket.as<unsigned int>());
     MF_LAUNCH_CK();
   }
 
   void enqueue_body(cudaStream_t s, cudaGraphConditionalHandle h, int set_handle) {
     dim3 ig(img_blocks(), ctx.B);
+    if (op->corrected()) {  // new FP64 anchor x_a = x every refresh_every outer iterations
+      k_copy_gated<<<ig, 256, 0, s>>>(ctx.xa, ctx.x, dm, ctx.st, kGateRefresh);
+      MF_LAUNCH_CK();
+      op->refresh_anchor(s, kGateRefresh);
+    }
     // gradient at z (only problems that start a new outer iteration)
     op->forward(s, ctx.z, kGateGrad, kQChiZ, true);
-    op->adjoint(s, form == kFormTSV ? ctx.z : nullptr, form == kFormTSV ? kQTsvZ : -1);
+    // the adjoint folds in the TSV gradient of z; TSV(z) itself is reduced by
+    // k_update_tsv with the same tree as TSV(xnew)
+    op->adjoint(s, form == kFormTSV ? ctx.z : nullptr, -1);
     // trial point
     if (form == kFormTSV) {
       k_update_tsv<<<ig, 256, 0, s>>>(ctx.z, ctx.dfdx, ctx.xnew, dm, ctx.prm, ctx.st, box_ptr, ctx.part);
@@ -862,8 +957,13 @@ struct Solver {
     MF_CK(cudaMemcpyAsync(ctx.z, ctx.x, bytes, cudaMemcpyDeviceToDevice, stream));
     k_init_state<<<cdiv(ctx.B, 128), 128, 0, stream>>>(ctx.st, ctx.B, 0);
     MF_LAUNCH_CK();
+    if (op->corrected()) {  // anchor = starting point
+      k_copy_gated<<<ig, 256, 0, stream>>>(ctx.xa, ctx.x, dm, ctx.st, kGateInit);
+      MF_LAUNCH_CK();
+      op->refresh_anchor(stream, kGateInit);
+    }
     if (!skip_loop) {
-      op->forward(stream, ctx.x, kGateInit, kQChiX, false);
+      op->forward_exact(stream, ctx.x, kGateInit, kQChiX, false);
       k_stats<<<ig, 256, 0, stream>>>(ctx.x, nullptr, nullptr, dm, ctx.prm, ctx.st, kGateInit, form, 0, 0, ctx.part);
       MF_LAUNCH_CK();
       launch_control(stream, kCtrlInit, 0, 0);
@@ -877,8 +977,8 @@ struct Solver {
         }
       }
     }
-    // summary at x (calc_result_*)
-    op->forward(stream, ctx.x, kGateAll, kQChiX, true);
+    // summary at x (calc_result_*), with the FP64 operator
+    op->forward_exact(stream, ctx.x, kGateAll, kQChiX, true);
     k_stats<<<ig, 256, 0, stream>>>(ctx.x, nullptr, nullptr, dm, ctx.prm, ctx.st, kGateAll, form, 1, 0, ctx.part);
     MF_LAUNCH_CK();
     launch_control(stream, kCtrlFinal, 0, 0);

@@ -53,13 +53,15 @@ def test_uneven_geometry_batch_equals_single_solves(gpulib, c0):
 
 
 def test_fp32_form_against_fp64(gpulib, c0):
+    """FP32 operators: the objective tracks FP64 to the FP32 floor (~1e-5
+    relative on this data: 1 % noise under the model values)."""
     probs = _problems(c0, [0.5, 1.0, 2.0, 8.0], 150)
     args = (c0["u"], c0["v"], c0["vis_r"], c0["vis_i"], c0["vis_std"], 64, 64, probs, 1e-5)
     X64, R64 = gpulib.nufft_batch(*args)
     X32, R32 = gpulib.nufft_batch(*args, precision=gpulib.FP32)
     for b in range(len(probs)):
-        assert rel(X32[b], X64[b]) < 1e-3
-        assert abs(R32[b]["finalcost"] - R64[b]["finalcost"]) <= 1e-6 * R64[b]["finalcost"]
+        assert rel(X32[b], X64[b]) < 1e-2
+        assert abs(R32[b]["finalcost"] - R64[b]["finalcost"]) <= 5e-5 * R64[b]["finalcost"]
 
 
 def test_plan_reuse_is_deterministic(gpulib, c0):
@@ -107,3 +109,20 @@ def test_batch_rejects_mixed_regularisers(gpulib, c0):
     probs[0]["lambda_tv"] = 1.0
     with pytest.raises(gpulib.MfistaError):
         gpulib.nufft_batch(c0["u"], c0["v"], c0["vis_r"], c0["vis_i"], c0["vis_std"], 64, 64, probs, 1e-5)
+
+
+def test_fp32_defect_corrected_reaches_fp64_objective(gpulib, c0):
+    """FP32 operators with the FP64 anchor correction reach the FP64
+    objective to 1e-6 relative (the uncorrected FP32 form stalls near 1e-5)."""
+    probs = _problems(c0, [0.5, 2.0], 1200)
+    geo = (c0["u"], c0["v"], c0["vis_r"], c0["vis_i"], c0["vis_std"], 64, 64)
+    X64, R64 = gpulib.nufft_batch(*geo, probs, 0.0)
+    targets = [r["finalcost"] * (1 + 1e-6) for r in R64]
+    for p, t in zip(probs, targets):
+        p["target_cost"] = t
+        p["maxiter"] = 4000
+    X32, R32 = gpulib.nufft_batch(*geo, probs, 0.0, precision=gpulib.FP32)
+    for b, (r, t) in enumerate(zip(R32, targets)):
+        assert r["finalcost"] <= t, (b, r["finalcost"], t)
+        assert r["ITER"] < 4000
+        assert rel(X32[b], X64[b]) < 2e-2

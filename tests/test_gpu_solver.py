@@ -138,3 +138,22 @@ def test_dft_raw_entry_point_allocates_residual(gpulib, c2):
     resid = np.ctypeslib.as_array(r.residual, shape=(m,)).copy()
     assert rel(resid, c2["tsv_resid"]) < 1e-7
     C.CDLL(None).free(C.cast(r.residual, C.c_void_p))
+
+
+def test_dft_batch_gemm_matches_reference(gpulib, c2):
+    """Three problems through the batched GEMM path; the one with the golden
+    parameters matches the reference's output."""
+    nx = int(c2["nx"])
+    lam1, cinit = float(c2["lam1"]), float(c2["cinit"])
+    probs = [dict(lambda_l1=lam1 * s, lambda_tsv=1e-3 * lam1 * s, cinit=cinit, maxiter=300, nonneg_flag=1)
+             for s in (0.5, 1.0, 3.0)]
+    X, R = gpulib.dft_batch(c2["y"], c2["A"], nx, nx, probs, 1e-6)
+    gold = res_dict(c2["tsv_res"])
+    assert R[1]["ITER"] == gold["ITER"]
+    assert rel(X[1], c2["tsv_x"]) < 1e-7
+    assert abs(R[1]["finalcost"] - gold["finalcost"]) <= 1e-10 * gold["finalcost"]
+    for b in (0, 2):
+        x, r = gpulib.imaging_core_dft(c2["y"], c2["A"], nx, nx, 300, 1e-6, probs[b]["lambda_l1"], 0.0,
+                                       probs[b]["lambda_tsv"], cinit)
+        assert R[b]["ITER"] == r["ITER"]
+        assert rel(X[b], x) < 1e-7
