@@ -12,10 +12,13 @@
 //     the half-plane grid and gathers the taps of the points binned to it, so
 //     there are no atomics and the result is deterministic.
 #pragma once
+#include <cooperative_groups.h>
 #include "common.cuh"
 #include "fft_smem.cuh"
 
 namespace mf {
+
+namespace cg = cooperative_groups;
 
 // Geometry of a batch of NUFFT problems (points concatenated).
 template <typename T> struct NufftGeom {
@@ -566,24 +569,35 @@ __global__ void __launch_bounds__(256, SharedChunk<T>::kInterpMinBlocks) k_nufft
   }
 }
 
-// spreading: one CTA per (16 x 16 tile, problem chunk), one thread per cell
-// holding the chunk's accumulators; the tile's points (taps, the chunk's
-// residuals and 16-bit masks of the tile rows / columns their direct or
-// mirrored footprint covers) are staged through shared memory and read as
+// spreading: one thread-block cluster per (16 x 16 tile, problem chunk); one
+// thread per cell holding the chunk's accumulators.  The tile's point list is
+// split into contiguous segments, one per CTA of the cluster, which bounds
+// the serial loop of the densest tiles; rank 0 then adds the segments'
+// accumulators from the other CTAs' shared memory (DSMEM) in rank order, so
+// the result is deterministic and no atomics are used.  Points (taps, the
+// chunk's residuals and 16-bit masks of the tile rows / columns their direct
+// or mirrored footprint covers) are staged through shared memory and read as
 // broadcasts, so a point that misses a cell costs one mask test.
+constexpr int kSpreadTile = 16;
+
 template <typename T>
 __global__ void __launch_bounds__(256, 2) k_nufft_spread_shared(NufftGeom<T> geo, const cplx<T>* __restrict__ y2,
-                                                             cplx<T>* __restrict__ gall, long gstride, int nx,
-                                                             int ny, int ntiles, const ProbState* __restrict__ st,
-                                                             int gate, int B) {
+                                                                cplx<T>* __restrict__ gall, long gstride, int nx,
+                                                                int ny, int ntiles, const ProbState* __restrict__ st,
+                                                                int gate, int B) {
   constexpr int PB = SharedChunk<T>::kSpread;
   constexpr int P = 32;
-  constexpr int TILE = 16;
+  constexpr int TILE = kSpreadTile;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* s_acc = reinterpret_cast<cplx<T>*>(smem_raw);  // [PB][256] segment accumulators
   __shared__ int s_ox[P], s_oy[P];          // 11 - mx, 11 - my
   __shared__ unsigned int s_mask[P];        // rows (low 16 bits) | cols (high 16 bits)
   __shared__ T s_wx[P][kTaps], s_wy[P][kTaps];
   __shared__ __align__(16) cplx<T> s_r[P][PB];
   __shared__ int s_act[PB];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const int csize = (int)cluster.num_blocks();
   const int b0 = blockIdx.y * PB;
   if (threadIdx.x < PB) {
     int b = b0 + threadIdx.x;
@@ -593,8 +607,8 @@ __global__ void __launch_bounds__(256, 2) k_nufft_spread_shared(NufftGeom<T> geo
   int any = 0;
 #pragma unroll
   for (int i = 0; i < PB; ++i) any |= s_act[i];
-  if (!any) return;
-  const int tile = blockIdx.x;
+  if (!any) return;  // uniform over the cluster: same problem chunk
+  const int tile = blockIdx.x / csize;
   const int ntc = (ny + 1 + TILE - 1) / TILE;
   const int tr = tile / ntc, tc = tile - tr * ntc;
   const int ty = threadIdx.x / TILE, tx = threadIdx.x - ty * TILE;
@@ -606,7 +620,9 @@ __global__ void __launch_bounds__(256, 2) k_nufft_spread_shared(NufftGeom<T> geo
   T ar[PB], ai[PB];
 #pragma unroll
   for (int i = 0; i < PB; ++i) ar[i] = ai[i] = 0;
-  const int beg = geo.tile_ptr[tile], end = geo.tile_ptr[tile + 1];
+  const int lbeg = geo.tile_ptr[tile], lend = geo.tile_ptr[tile + 1];
+  const int seg = (lend - lbeg + csize - 1) / csize;
+  const int beg = min(lend, lbeg + rank * seg), end = min(lend, beg + seg);
   for (int c0 = beg; c0 < end; c0 += P) {
     const int np = min(P, end - c0);
     __syncthreads();
@@ -677,11 +693,27 @@ __global__ void __launch_bounds__(256, 2) k_nufft_spread_shared(NufftGeom<T> geo
       }
     }
   }
-  if (valid) {
+  // segment accumulators -> shared memory; rank 0 adds ranks 1.. in order
 #pragma unroll
-    for (int i = 0; i < PB; ++i)
-      if (s_act[i]) gall[(size_t)(b0 + i) * gstride + (size_t)row * (ny + 1) + col] = mk<T>(ar[i], ai[i]);
+  for (int i = 0; i < PB; ++i) s_acc[i * 256 + threadIdx.x] = mk<T>(ar[i], ai[i]);
+  cluster.sync();
+  if (rank == 0) {
+    for (int r = 1; r < csize; ++r) {
+      const cplx<T>* peer = cluster.map_shared_rank(s_acc, r);
+#pragma unroll
+      for (int i = 0; i < PB; ++i) {
+        cplx<T> v = peer[i * 256 + threadIdx.x];
+        ar[i] += v.x;
+        ai[i] += v.y;
+      }
+    }
+    if (valid) {
+#pragma unroll
+      for (int i = 0; i < PB; ++i)
+        if (s_act[i]) gall[(size_t)(b0 + i) * gstride + (size_t)row * (ny + 1) + col] = mk<T>(ar[i], ai[i]);
+    }
   }
+  cluster.sync();  // peers' shared memory must stay alive until rank 0 is done
 }
 
 }  // namespace mf

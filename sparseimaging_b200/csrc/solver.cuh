@@ -292,6 +292,7 @@ template <typename T> struct NufftOp : Op {
     set_smem(k_nufft_rows_fwd<T>, smem_rows);
     set_smem(k_nufft_rows_inv<T>, smem_rows);
     set_smem(k_nufft_cols<T>, smem_cols);
+    set_smem(k_nufft_spread_shared<T>, spread_smem());
     if (correct && sizeof(T) == 4) {
       exact.reset(new NufftOp<double>(ctx, in, false));
       d_axa.alloc(sizeof(double2) * (size_t)y2n);
@@ -316,6 +317,8 @@ template <typename T> struct NufftOp : Op {
 
   int interp_blocks() const { return std::max(1, cdiv(mmax, shared ? 8 * kInterpPtsPerWarp : 8)); }
   int interp_chunks() const { return cdiv(B, SharedChunk<T>::kInterp); }
+  static constexpr int kSpreadCluster = 8;
+  static size_t spread_smem() { return sizeof(cplx<T>) * SharedChunk<T>::kSpread * 256; }
   int spread_chunks() const { return cdiv(B, SharedChunk<T>::kSpread); }
 
   void launch_interp(cudaStream_t s, cplx<T>* g, int gate, int qchi, cplx<T>* y2, const double2* base = nullptr,
@@ -360,9 +363,24 @@ template <typename T> struct NufftOp : Op {
   }
 
   void launch_spread(cudaStream_t s, cplx<T>* g, int gate) {
-    if (shared)
-      k_nufft_spread_shared<T><<<dim3(ntiles, spread_chunks()), 256, 0, s>>>(geo, d_y2.as<cplx<T>>(), g, gstride, nx,
-                                                                             ny, ntiles, c.st, gate, B);
+    if (shared) {
+      // cluster of kSpreadCluster CTAs per tile, each a segment of its points
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(ntiles * kSpreadCluster, spread_chunks(), 1);
+      cfg.blockDim = dim3(256, 1, 1);
+      cfg.dynamicSmemBytes = spread_smem();
+      cfg.stream = s;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = kSpreadCluster;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      MF_CK(cudaLaunchKernelEx(&cfg, k_nufft_spread_shared<T>, geo, (const cplx<T>*)d_y2.as<cplx<T>>(), g, gstride,
+                               nx, ny, ntiles, (const ProbState*)c.st, gate, B));
+      return;
+    }
     else
       k_nufft_spread<T><<<dim3(ntiles, B), tile_r * tile_c, 0, s>>>(geo, d_y2.as<cplx<T>>(), g, gstride, nx, ny,
                                                                     tile_r, tile_c, ntiles, c.st, gate);
