@@ -68,6 +68,10 @@ def workload(seed):
     return synth.lambda_grid_problem(seed=seed, nx=NX, n_stations=N_STATIONS, n_hours=N_HOURS)
 
 
+def workload_name(nx, m, b):
+    return f"NUFFT {nx}x{nx}, M={m}, {b}-problem lambda grid (8x8 log, 1e-4..1 of max|A^H y|)"
+
+
 def peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -359,7 +363,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 operators + f64 defect correction, f64 objective" if chosen_prec == si.FP32 else "f64",
             "data": "synthetic (seeded sky + uv coverage, rank-seeded)",
-            "config": {"workload": f"NUFFT {nx}x{nx}, M={M}, {B}-problem lambda grid (8x8 log, 1e-4..1 of max|A^H y|)",
+            "config": {"workload": workload_name(nx, M, B),
                        "method": ("batched, FP32 NUFFT/FFT with FP64 anchor correction" if chosen_prec == si.FP32 else "batched FP64") + ", device-resident CUDA-graph loop, per-problem stop at F*(1+1e-6)",
                        "l2": "flushed between steps (512 MB write)", "fstar": fstar_src,
                        "parallelism": f"replicas x{world}"},
@@ -406,8 +410,9 @@ def run_reference(args):
     v = float(np.mean([s["value"] for s in steps]))
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 5), "unit": "solves/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 operators + f64 defect correction, f64 objective" if chosen_prec == si.FP32 else "f64", "data": "synthetic",
-            "config": {"workload": f"NUFFT {NX}x{NX}, M={p.m}, 64-problem lambda grid (8x8 log, 1e-4..1 of max|A^H y|)"},
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sky + uv coverage)",
+            "config": {"workload": workload_name(p.nx, p.m, len(grid)),
+                       "method": "reference C MFISTA (FFTW/BLAS stand-ins), one problem per process"},
             "cpu_baseline": {"value": round(v, 5), "unit": "solves/s", "cores": steps[0]["cores"],
                              "kind": "reference", "sample": steps[0]["sample"]},
             "e2e": {"value": round(v, 5), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
