@@ -196,6 +196,27 @@ int mfista_nufft_forward(const double *u_dx, const double *v_dy, int M, int Nx, 
 int mfista_nufft_adjoint(const double *u_dx, const double *v_dy, int M, int Nx, int Ny,
                          const double *r_r, const double *r_i, double *x_out, int precision);
 
+/* NUFFT forward operator for callers that may not allocate GPU memory (no
+ * counterpart in the reference).  Meant for hosts whose device memory is
+ * owned by their own pool, or that cannot take the device-wide
+ * synchronisation a cudaMalloc/cudaFree brings; mfista_nufft_forward
+ * allocates its working buffers on every call.
+ *   u_dx, v_dy [M], x [Nx*Ny], out_r, out_i [M]: DEVICE pointers; FP64.
+ *   stream: a cudaStream_t (NULL: the default stream); the work is enqueued
+ *           there and the call returns without waiting for it.
+ * All intermediates live in one fixed device array of
+ * MFISTA_NOALLOC_SCRATCH_BYTES, which a device holds from the first call on
+ * it (earlier where CUDA loads modules eagerly) until the process exits;
+ * nothing is allocated or freed.  Inputs whose working set (about 32*Nx*(Ny+1) + 8*Nx*Ny + 408*M bytes) exceeds it, and
+ * Nx > 767 or Ny > 1535, are rejected with MFISTA_ERR_ARG.  The first call
+ * on a device looks up the array's address there: make it before any stream
+ * capture.  Calls share the array, so calls that may run at the same time on
+ * one GPU race and must be ordered by the caller.  Returns an mfista_status;
+ * mfista_last_status/error are not updated. */
+#define MFISTA_NOALLOC_SCRATCH_BYTES (16u << 20)
+int mfista_nufft_forward_noalloc(const double *u_dx, const double *v_dy, int M, int Nx, int Ny,
+                                 const double *x, double *out_r, double *out_i, void *stream);
+
 /* FGP TV proximal map alone (FGP_L1_box / FGP_nonneg_box,
  * c/mfista_TV_lib.c:189-384) on an NX x NY view: x_out = prox(b). */
 int mfista_fgp_prox(const double *b, int NX, int NY, double lambda_l1, double lambda_tv,

@@ -92,7 +92,7 @@ __global__ void k_nufft_prep_points(const double* __restrict__ u, const double* 
   }
 }
 
-__global__ void k_nufft_prep_e4(double* __restrict__ e4, int nx, int ny) {
+static __global__ void k_nufft_prep_e4(double* __restrict__ e4, int nx, int ny) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nx * ny) return;
   int i = t / ny, j = t - i * ny;
