@@ -114,7 +114,11 @@ int mfista_set_fgp_iter(int n);
 
 /* Arithmetic of the operators (spread/interp/FFT/stencils).  The objective,
  * reductions, backtracking test and FISTA sequence are FP64 in both. */
-enum mfista_precision { MFISTA_FP64 = 64, MFISTA_FP32 = 32 };
+enum mfista_precision { MFISTA_FP64 = 64, MFISTA_FP32 = 32, MFISTA_BF16X3 = 3 };
+/* MFISTA_BF16X3 (DFT operator only): A z and A^T r on the tensor cores as
+ * three BF16 products of split operands (hi*hi + hi*lo + lo*hi) with FP32
+ * accumulation, applied to the departure from an FP64 anchor that is
+ * refreshed every 32 outer iterations, so results keep FP64 accuracy. */
 
 /* Per-problem parameters of a batched solve. */
 struct mfista_problem {
@@ -179,6 +183,24 @@ void *mfista_plan_stream(mfista_plan plan);          /* cudaStream_t */
 int mfista_plan_profile(mfista_plan plan, int kernel, int reps, double *ms_per_launch,
                         double *bytes_per_launch);
 int mfista_plan_kernel_launches(mfista_plan plan);   /* kernels per solve, last run */
+/* Launch shapes of the plan's operator kernels, as int[4]:
+ *   [0] interpolation points per warp (shared geometry; 1..32),
+ *   [1] spreading CTAs per tile cluster (shared geometry; 1..16),
+ *   [2] image rows per CTA of the row FFT passes,
+ *   [3] grid columns per CTA of the column FFT passes;
+ * 0 = not used by this plan's operator (get) or keep the current value
+ * (set).  Rows/columns per CTA leave results bit-identical; the other two
+ * regroup sums and move results by rounding only.  set_shapes captures the
+ * solve graph again; an impossible shape returns MFISTA_ERR_ARG. */
+int mfista_plan_get_shapes(mfista_plan plan, int *shapes);
+int mfista_plan_set_shapes(mfista_plan plan, const int *shapes);
+/* Autotuner: times every candidate shape of each knob above with the
+ * plan's kernels in isolation (as mfista_plan_profile, `reps` launches),
+ * one knob at a time, keeps the fastest, and captures the graph again.
+ * shapes_out: int[4] chosen shapes; ms_out: double[4] best time per launch
+ * of each knob's kernels (0 for unused knobs).  Either may be NULL.  Like
+ * mfista_plan_profile, it leaves the iterates undefined. */
+int mfista_plan_tune(mfista_plan plan, int reps, int *shapes_out, double *ms_out);
 /* Per-problem status of the last fetched solve (enum mfista_status values). */
 int mfista_plan_statuses(mfista_plan plan, int *status_out);
 /* 1 when the plan iterates with a device-side conditional WHILE graph node,
@@ -216,6 +238,15 @@ int mfista_nufft_adjoint(const double *u_dx, const double *v_dy, int M, int Nx, 
 #define MFISTA_NOALLOC_SCRATCH_BYTES (16u << 20)
 int mfista_nufft_forward_noalloc(const double *u_dx, const double *v_dy, int M, int Nx, int Ny,
                                  const double *x, double *out_r, double *out_i, void *stream);
+
+/* DFT operator alone for B vectors (dgemv "N"/"T" of c/mfista_dft_lib.c:30-66,
+ * :253-278, batched): A is column-major M x N;
+ *   transpose = 0: out[b][m] = sum_n A[m + n M] X[b][n]   (X [B][N], out [B][M])
+ *   transpose = 1: out[b][n] = sum_m A[m + n M] X[b][m]   (X [B][M], out [B][N])
+ * precision MFISTA_FP64, or MFISTA_BF16X3 for the tensor-core split-BF16
+ * GEMM alone (no anchor: ~1e-5 relative error). */
+int mfista_dft_apply(const double *A, int M, int N, const double *X, int B, int transpose, int precision,
+                     double *out);
 
 /* FGP TV proximal map alone (FGP_L1_box / FGP_nonneg_box,
  * c/mfista_TV_lib.c:189-384) on an NX x NY view: x_out = prox(b). */

@@ -118,6 +118,13 @@ def lib():
         L.mfista_plan_kernel_launches.argtypes = [C.c_void_p]
         L.mfista_plan_profile.restype = C.c_int
         L.mfista_plan_profile.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp]
+        _i4 = C.POINTER(C.c_int)
+        L.mfista_plan_get_shapes.restype = C.c_int
+        L.mfista_plan_get_shapes.argtypes = [C.c_void_p, _i4]
+        L.mfista_plan_set_shapes.restype = C.c_int
+        L.mfista_plan_set_shapes.argtypes = [C.c_void_p, _i4]
+        L.mfista_plan_tune.restype = C.c_int
+        L.mfista_plan_tune.argtypes = [C.c_void_p, C.c_int, _i4, _dp]
         L.mfista_plan_destroy.restype = None
         L.mfista_plan_destroy.argtypes = [C.c_void_p]
         L.mfista_nufft_forward.restype = C.c_int
@@ -360,6 +367,32 @@ class Plan:
         ms, by = C.c_double(0), C.c_double(0)
         _check(lib().mfista_plan_profile(self.h, kernel, reps, C.byref(ms), C.byref(by)))
         return ms.value, by.value
+
+    SHAPE_KEYS = ("interp_ppw", "spread_cluster", "rows_per_cta", "cols_per_cta")
+
+    def shapes(self):
+        """Launch shapes of the operator kernels (0 = not used by this plan)."""
+        a = (C.c_int * 4)()
+        _check(lib().mfista_plan_get_shapes(self.h, a))
+        return dict(zip(self.SHAPE_KEYS, list(a)))
+
+    def set_shapes(self, **shapes):
+        """Sets some launch shapes (the others keep their value) and captures
+        the solve graph again."""
+        unknown = set(shapes) - set(self.SHAPE_KEYS)
+        if unknown:
+            raise ValueError(f"unknown shape keys {sorted(unknown)}")
+        a = (C.c_int * 4)(*[int(shapes.get(k, 0)) for k in self.SHAPE_KEYS])
+        _check(lib().mfista_plan_set_shapes(self.h, a))
+
+    def tune(self, reps=10):
+        """Autotunes the launch shapes on this GPU; returns (shapes, best ms
+        per launch of each knob's kernels).  Iterates are left undefined:
+        call set_problems before the next run."""
+        a = (C.c_int * 4)()
+        ms = np.zeros(4)
+        _check(lib().mfista_plan_tune(self.h, reps, a, _p(ms)))
+        return dict(zip(self.SHAPE_KEYS, list(a))), dict(zip(self.SHAPE_KEYS, ms.tolist()))
 
     @property
     def stream(self):

@@ -224,3 +224,71 @@ __global__ void k_dft_atr_finish(DftGeom g, const double* __restrict__ atr_part,
 }
 
 }  // namespace mf
+
+// ===========================================================================
+// Split-BF16 tensor-core form (tc::k_gemm_bf16x3) with FP64 defect
+// correction: for an anchor x_a (refreshed in FP64 every few outer
+// iterations) with ax_a = A x_a, r_a = y - ax_a and g_a = A^T r_a,
+//   A v   = ax_a + A (v - x_a)            (tensor-core part: A (v - x_a))
+//   A^T r = g_a  + A^T (r - r_a)          (tensor-core part: A^T (r - r_a))
+// so the low-precision products only carry the (small) departures from the
+// anchor.  Partials arrive per K split as FP32 [nsplit][bpad][rows] and are
+// summed in a fixed order in FP64.
+// ===========================================================================
+namespace mf {
+
+// r = y - (ax_a + sum_s part[s]) ; chi^2 partials; r stored when `store`
+__global__ void k_dft_tc_resid(const float* __restrict__ part, int nsplit, int bpad, int rows,
+                               const double* __restrict__ axa, DftGeom g, const ProbState* __restrict__ st, int gate,
+                               Partials pq, int qchi, int store) {
+  __shared__ double sh[32];
+  int b = blockIdx.y;
+  if (!gate_ok(st[b], gate)) return;
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[1] = {0.0};
+  if (m < g.M) {
+    double s = axa[(size_t)b * g.M + m];
+    for (int k = 0; k < nsplit; ++k) s += (double)part[((size_t)k * bpad + b) * rows + m];
+    double r = g.y[m] - s;
+    acc[0] = r * r;
+    if (store) g.resid[(size_t)b * g.M + m] = r;
+  }
+  block_sum<1>(acc, sh);
+  if (threadIdx.x == 0 && qchi >= 0) pq.at(qchi, b)[blockIdx.x] = acc[0];
+}
+
+// dfdx[n] = beta dTSV(z)[n] + g_a[n] + sum_s part[s][n]   (beta = -lambda_tsv or 0)
+__global__ void k_dft_tc_atr_finish(const float* __restrict__ part, int nsplit, int bpad, int rows,
+                                    const double* __restrict__ ga, int N, double* __restrict__ dall, long xstride,
+                                    const double* __restrict__ zall, const ProbParams* __restrict__ prm, int tsvNX,
+                                    int tsvNY, const ProbState* __restrict__ st, int gate) {
+  int b = blockIdx.y;
+  if (!gate_ok(st[b], gate)) return;
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  double s = ga[(size_t)b * N + n];
+  for (int k = 0; k < nsplit; ++k) s += (double)part[((size_t)k * bpad + b) * rows + n];
+  const ProbParams& pp = prm[b];
+  double* d = dall + (size_t)b * xstride;
+  if (zall != nullptr && pp.lambda_tsv > 0.0) {
+    const double* z = zall + (size_t)b * xstride;
+    d[n] = dtsv_at(z, n, tsvNX, tsvNY) * (-pp.lambda_tsv) + s;
+  } else {
+    d[n] = s;
+  }
+}
+
+// anchor model from the FP64 GEMM partials: ax_a = sum_c az_part, r_a = y - ax_a
+__global__ void k_dft_anchor(DftGeom g, const ProbState* __restrict__ st, int gate, double* __restrict__ axa,
+                             double* __restrict__ ra) {
+  int b = blockIdx.y;
+  if (!gate_ok(st[b], gate)) return;
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= g.M) return;
+  double s = 0.0;
+  for (int c = 0; c < g.nchunk; ++c) s += g.az_part[((size_t)b * g.nchunk + c) * g.M + m];
+  axa[(size_t)b * g.M + m] = s;
+  ra[(size_t)b * g.M + m] = g.y[m] - s;
+}
+
+}  // namespace mf

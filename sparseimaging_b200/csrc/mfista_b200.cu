@@ -389,6 +389,55 @@ extern "C" int mfista_plan_profile(mfista_plan P, int kernel, int reps, double* 
     return fail(e.status, e.what(), false);
   }
 }
+extern "C" int mfista_plan_get_shapes(mfista_plan P, int* shapes) {
+  set_ok();
+  if (!P || !shapes) return fail(MFISTA_ERR_ARG, "null argument", false);
+  LaunchShapes sh = P->S->op->shapes();
+  shapes[0] = sh.interp_ppw;
+  shapes[1] = sh.spread_cluster;
+  shapes[2] = sh.rows_per_cta;
+  shapes[3] = sh.cols_per_cta;
+  return MFISTA_OK;
+}
+
+extern "C" int mfista_plan_set_shapes(mfista_plan P, const int* shapes) {
+  set_ok();
+  if (!P || !shapes) return fail(MFISTA_ERR_ARG, "null argument", false);
+  try {
+    LaunchShapes sh;
+    sh.interp_ppw = shapes[0];
+    sh.spread_cluster = shapes[1];
+    sh.rows_per_cta = shapes[2];
+    sh.cols_per_cta = shapes[3];
+    if (sh.spread_cluster && P->S->op->shapes().spread_cluster && !P->S->spread_cluster_fits(sh.spread_cluster))
+      throw Error(MFISTA_ERR_ARG, "spread cluster of " + std::to_string(sh.spread_cluster) + " CTAs cannot be resident");
+    P->S->apply_shapes(sh);
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
+extern "C" int mfista_plan_tune(mfista_plan P, int reps, int* shapes_out, double* ms_out) {
+  set_ok();
+  if (!P) return fail(MFISTA_ERR_ARG, "null plan", false);
+  try {
+    double ms[4] = {0, 0, 0, 0};
+    LaunchShapes sh = P->S->tune(std::max(1, reps), ms);
+    if (shapes_out) {
+      shapes_out[0] = sh.interp_ppw;
+      shapes_out[1] = sh.spread_cluster;
+      shapes_out[2] = sh.rows_per_cta;
+      shapes_out[3] = sh.cols_per_cta;
+    }
+    if (ms_out)
+      for (int k = 0; k < 4; ++k) ms_out[k] = ms[k];
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
 extern "C" int mfista_plan_kernel_launches(mfista_plan P) { return P ? P->launches : 0; }
 extern "C" int mfista_plan_statuses(mfista_plan P, int* status_out) {
   if (!P) return MFISTA_ERR_ARG;
@@ -423,7 +472,8 @@ extern "C" int mfista_dft_batch(const double* y, const double* A, int M, int N, 
   set_ok();
   try {
     if (B < 1) throw Error(MFISTA_ERR_ARG, "B must be >= 1");
-    if (precision != MFISTA_FP64) throw Error(MFISTA_ERR_ARG, "the batched DFT runs in FP64");
+    if (precision != MFISTA_FP64 && precision != MFISTA_BF16X3)
+      throw Error(MFISTA_ERR_ARG, "the batched DFT runs in FP64 or BF16X3");
     int form = problems[0].lambda_tv != 0 ? kFormTV : kFormTSV;
     std::vector<ProbParams> prm(B);
     for (int b = 0; b < B; ++b) {
@@ -439,13 +489,14 @@ extern "C" int mfista_dft_batch(const double* y, const double* A, int M, int N, 
     Solver S;
     S.precision = MFISTA_FP64;
     S.init_common(B, N, NX, NY, form, fgp_iter, nullptr);
-    S.op.reset(new DftOp(S.ctx, A, y, M, N));
+    S.op.reset(new DftOp(S.ctx, A, y, M, N, precision));
     S.finish_setup();
     double t0 = now_s();
     S.upload_problems(prm, xinit);
     S.enqueue_solve(false);
     std::vector<FinalOut> o;
     S.fetch(xout, o);
+    if (S.op->device_error()) throw Error(MFISTA_ERR_CUDA, "a tensor-core GEMM wait timed out");
     double ct = now_s() - t0;
     int worst = 0;
     for (int b = 0; b < B; ++b) {
@@ -534,6 +585,51 @@ extern "C" int mfista_nufft_adjoint(const double* u_dx, const double* v_dy, int 
     if (precision == MFISTA_FP32)
       return nufft_apply<float>(u_dx, v_dy, nullptr, M, Nx, Ny, nullptr, r_r, r_i, nullptr, nullptr, x_out);
     return nufft_apply<double>(u_dx, v_dy, nullptr, M, Nx, Ny, nullptr, r_r, r_i, nullptr, nullptr, x_out);
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
+extern "C" int mfista_dft_apply(const double* A, int M, int N, const double* X, int B, int transpose, int precision,
+                                double* out) {
+  set_ok();
+  try {
+    if (M < 1 || N < 1 || B < 1 || !A || !X || !out) throw Error(MFISTA_ERR_ARG, "bad sizes or null pointer");
+    Solver S;
+    S.precision = MFISTA_FP64;
+    S.init_common(B, N, N, 1, kFormTSV, 100, nullptr);
+    std::vector<double> y(M, 0.0);
+    DftOp* op = new DftOp(S.ctx, A, y.data(), M, N, precision);
+    S.op.reset(op);
+    int slots = std::max({op->chi_slots(), op->tsv_slots(), 1});
+    S.d_part.alloc(sizeof(double) * (size_t)kNumQ * B * slots);
+    S.ctx.part.p = S.d_part.as<double>();
+    S.ctx.part.slots = slots;
+    S.ctx.part.B = B;
+    std::vector<ProbState> st(B);
+    for (ProbState& q : st) {
+      memset(&q, 0, sizeof(q));
+      q.active = 1;
+      q.need_grad = 1;
+    }
+    MF_CK(cudaMemcpy(S.ctx.st, st.data(), sizeof(ProbState) * B, cudaMemcpyHostToDevice));
+    MF_CK(cudaMemset(S.ctx.prm, 0, sizeof(ProbParams) * B));
+    MF_CK(cudaMemset(S.ctx.xa, 0, sizeof(double) * (size_t)B * N));  // anchor 0: the whole product is A x
+    if (!transpose) {
+      MF_CK(cudaMemcpy(S.ctx.x, X, sizeof(double) * (size_t)B * N, cudaMemcpyHostToDevice));
+      op->forward(S.stream, S.ctx.x, kGateAll, kQChiX, true);  // stores y - A x with y = 0
+      std::vector<double> r((size_t)B * M);
+      MF_CK(cudaMemcpyAsync(r.data(), op->g.resid, sizeof(double) * r.size(), cudaMemcpyDeviceToHost, S.stream));
+      MF_CK(cudaStreamSynchronize(S.stream));
+      for (size_t i = 0; i < r.size(); ++i) out[i] = -r[i];
+    } else {
+      MF_CK(cudaMemcpy(op->g.resid, X, sizeof(double) * (size_t)B * M, cudaMemcpyHostToDevice));
+      op->adjoint(S.stream, nullptr, -1);
+      MF_CK(cudaMemcpyAsync(out, S.ctx.dfdx, sizeof(double) * (size_t)B * N, cudaMemcpyDeviceToHost, S.stream));
+      MF_CK(cudaStreamSynchronize(S.stream));
+    }
+    if (op->device_error()) throw Error(MFISTA_ERR_CUDA, "a tensor-core GEMM wait timed out");
+    return MFISTA_OK;
   } catch (const Error& e) {
     return fail(e.status, e.what(), false);
   }

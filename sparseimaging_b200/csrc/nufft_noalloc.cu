@@ -221,9 +221,10 @@ extern "C" int mfista_nufft_forward_noalloc(const double* u_dx, const double* v_
   Partials none;
   memset(&none, 0, sizeof(none));
   none.B = 1;
-  k_nufft_interp_shared<double><<<dim3(cdiv_i(M, 8 * kInterpPtsPerWarp), 1), T, 0, s>>>(
+  constexpr int ppw = SharedChunk<double>::kInterpPts;
+  k_nufft_interp_shared<double><<<dim3(cdiv_i(M, 8 * ppw), 1), T, 0, s>>>(
       geo, grid, 0, Nx, Ny, 1.0 / ((double)(2 * Nx) * (double)(2 * Ny)), st, kGateAll, none, -1, nullptr, 1, nullptr,
-      ax);
+      ax, ppw);
   k_noalloc_split<<<cdiv_i(M, T), T, 0, s>>>(ax, M, out_r, out_i);
   return cudaGetLastError() == cudaSuccess ? MFISTA_OK : MFISTA_ERR_CUDA;
 }

@@ -456,16 +456,20 @@ template <> struct SharedChunk<float> {
   static constexpr int kInterp = 16;  // problems per interpolation CTA
   static constexpr int kSpread = 16;  // problems per spreading CTA
   static constexpr int kInterpMinBlocks = 2;
+  static constexpr int kInterpPts = 2;  // default points per warp
 };
 template <> struct SharedChunk<double> {
   static constexpr int kInterp = 8;
   static constexpr int kSpread = 8;
   static constexpr int kInterpMinBlocks = 2;
+  static constexpr int kInterpPts = 8;
 };
 
 // interpolation: one warp per point, lanes over the 576 taps (18 each) with
-// cell and weight held in registers, looping over the CTA's problem chunk
-constexpr int kInterpPtsPerWarp = 8;
+// cell and weight held in registers, looping over the CTA's problem chunk;
+// each warp takes `ppw` consecutive points (a launch-shape choice: the
+// per-point arithmetic does not depend on it, the grouping of the chi^2
+// partial sums does)
 
 template <typename T>
 __global__ void __launch_bounds__(256, SharedChunk<T>::kInterpMinBlocks) k_nufft_interp_shared(NufftGeom<T> geo, const cplx<T>* __restrict__ gall,
@@ -473,7 +477,7 @@ __global__ void __launch_bounds__(256, SharedChunk<T>::kInterpMinBlocks) k_nufft
                                                              const ProbState* __restrict__ st, int gate,
                                                              Partials part, int qchi, cplx<T>* __restrict__ y2,
                                                              int B, const double2* __restrict__ ax_base,
-                                                             double2* __restrict__ ax_out) {
+                                                             double2* __restrict__ ax_out, int ppw) {
   constexpr int PB = SharedChunk<T>::kInterp;
   constexpr int NT = (kTaps * kTaps) / 32;
   __shared__ double s_chi[8][PB];
@@ -492,8 +496,8 @@ __global__ void __launch_bounds__(256, SharedChunk<T>::kInterpMinBlocks) k_nufft
   const int mtot = geo.pt_hi[0];
   if (lane < PB) s_chi[warp][lane] = 0.0;
   __syncwarp();
-  for (int q = 0; q < kInterpPtsPerWarp; ++q) {
-    const int k = (blockIdx.x * 8 + warp) * kInterpPtsPerWarp + q;
+  for (int q = 0; q < ppw; ++q) {
+    const int k = (blockIdx.x * 8 + warp) * ppw + q;
     if (k >= mtot) break;
     int cell[NT];
     T wgt[NT];

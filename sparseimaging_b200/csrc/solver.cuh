@@ -12,12 +12,14 @@
 
 #include <algorithm>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
 #include "common.cuh"
 #include "dft_ops.cuh"
+#include "dft_tc.cuh"
 #include "fft_smem.cuh"
 #include "fftvar_ops.cuh"
 #include "fgp.cuh"
@@ -104,9 +106,15 @@ template <typename T> struct FftHost {
   }
 };
 
+// Raises a kernel's dynamic shared-memory limit to at least `bytes`.  The
+// limit is per kernel and process-wide, so it is never lowered: another plan
+// may have captured launches that need more.
 template <typename K> void set_smem(K kernel, size_t bytes) {
   if (bytes > 227 * 1024) throw Error(MFISTA_ERR_ARG, "grid too large for the shared-memory FFT");
-  MF_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  cudaFuncAttributes fa;
+  MF_CK(cudaFuncGetAttributes(&fa, kernel));
+  if ((size_t)fa.maxDynamicSharedSizeBytes < bytes)
+    MF_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
 // ---------------------------------------------------------------------------
@@ -127,6 +135,18 @@ struct Ctx {
   Partials part{};
 };
 
+// Launch shapes of the operator kernels that the autotuner may change.
+//   interp_ppw:     points per warp of the shared-geometry interpolation
+//   spread_cluster: CTAs per tile cluster of the shared-geometry spreading
+//   rows_per_cta:   image rows per CTA of the row FFT passes
+//   cols_per_cta:   grid columns per CTA of the column FFT passes
+// 0 means "not used by this operator".  Row/column shapes leave every
+// result bit-identical; the interpolation and spreading shapes regroup sums
+// (chi^2 partials; spreading segments), which moves results by rounding only.
+struct LaunchShapes {
+  int interp_ppw = 0, spread_cluster = 0, rows_per_cta = 0, cols_per_cta = 0;
+};
+
 struct Op {
   virtual ~Op() {}
   // chi^2 partials of `src` into part[qchi]; `store` keeps the weighted
@@ -135,7 +155,12 @@ struct Op {
   // gradient at z into ctx.dfdx (gate: need_grad); TSV fused when z_tsv != 0
   virtual void adjoint(cudaStream_t s, const double* z_tsv, int qtsv) = 0;
   virtual int chi_slots() const = 0;
+  // largest chi_slots() over every launch shape set_shapes() accepts
+  virtual int max_chi_slots() const { return chi_slots(); }
   virtual int tsv_slots() const = 0;
+  virtual LaunchShapes shapes() const { return LaunchShapes(); }
+  // throws Error(MFISTA_ERR_ARG) for a shape the operator cannot run
+  virtual void set_shapes(const LaunchShapes& sh) { (void)sh; }
   virtual double fscale() const = 0;
   virtual int launches_forward() const = 0;
   virtual int launches_adjoint() const = 0;
@@ -152,6 +177,8 @@ struct Op {
     forward(s, src, gate, qchi, store);
   }
   virtual int launches_refresh() const { return 0; }
+  // non-zero when a device-side wait of the operator's kernels gave up
+  virtual int device_error() { return 0; }
 };
 
 // ---------------------------------------------------------------------------
@@ -205,6 +232,8 @@ template <typename T> struct NufftOp : Op {
   FftHost<T> fh, fcol;
   NufftGeom<T> geo{};
   int rpc = 8, cpc = 8, tile_r = 8, tile_c = 32, ntiles = 0;
+  int ippw = SharedChunk<T>::kInterpPts;  // interpolation points per warp (shared geometry)
+  int spread_cs = 8;                      // spreading cluster size (shared geometry)
   size_t smem_rows = 0, smem_cols = 0;
   long gstride = 0;
   double inv_mm = 0;
@@ -293,8 +322,10 @@ template <typename T> struct NufftOp : Op {
     set_smem(k_nufft_rows_inv<T>, smem_rows);
     set_smem(k_nufft_cols<T>, smem_cols);
     set_smem(k_nufft_spread_shared<T>, spread_smem());
+    MF_CK(cudaFuncSetAttribute(k_nufft_spread_shared<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     if (correct && sizeof(T) == 4) {
       exact.reset(new NufftOp<double>(ctx, in, false));
+      exact->ippw = ippw;  // its chi^2 partials land in the same slots as ours
       d_axa.alloc(sizeof(double2) * (size_t)y2n);
       MF_CK(cudaMemset(d_axa.p, 0, d_axa.bytes));
     }
@@ -315,9 +346,9 @@ template <typename T> struct NufftOp : Op {
     MF_CK(cudaDeviceSynchronize());
   }
 
-  int interp_blocks() const { return std::max(1, cdiv(mmax, shared ? 8 * kInterpPtsPerWarp : 8)); }
+  int interp_blocks() const { return std::max(1, cdiv(mmax, shared ? 8 * ippw : 8)); }
   int interp_chunks() const { return cdiv(B, SharedChunk<T>::kInterp); }
-  static constexpr int kSpreadCluster = 8;
+  static constexpr int kMaxInterpPpw = 32;
   static size_t spread_smem() { return sizeof(cplx<T>) * SharedChunk<T>::kSpread * 256; }
   int spread_chunks() const { return cdiv(B, SharedChunk<T>::kSpread); }
 
@@ -325,7 +356,7 @@ template <typename T> struct NufftOp : Op {
                      double2* out = nullptr) {
     if (shared)
       k_nufft_interp_shared<T><<<dim3(interp_blocks(), interp_chunks()), 256, 0, s>>>(
-          geo, g, gstride, nx, ny, inv_mm, c.st, gate, c.part, qchi, y2, B, base, out);
+          geo, g, gstride, nx, ny, inv_mm, c.st, gate, c.part, qchi, y2, B, base, out, ippw);
     else
       k_nufft_interp<T><<<dim3(interp_blocks(), B), 256, 0, s>>>(geo, g, gstride, nx, ny, inv_mm, c.st, gate,
                                                                  c.part, qchi, y2, base, out);
@@ -364,15 +395,15 @@ template <typename T> struct NufftOp : Op {
 
   void launch_spread(cudaStream_t s, cplx<T>* g, int gate) {
     if (shared) {
-      // cluster of kSpreadCluster CTAs per tile, each a segment of its points
+      // cluster of spread_cs CTAs per tile, each a segment of its points
       cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(ntiles * kSpreadCluster, spread_chunks(), 1);
+      cfg.gridDim = dim3(ntiles * spread_cs, spread_chunks(), 1);
       cfg.blockDim = dim3(256, 1, 1);
       cfg.dynamicSmemBytes = spread_smem();
       cfg.stream = s;
       cudaLaunchAttribute attr[1];
       attr[0].id = cudaLaunchAttributeClusterDimension;
-      attr[0].val.clusterDim.x = kSpreadCluster;
+      attr[0].val.clusterDim.x = spread_cs;
       attr[0].val.clusterDim.y = 1;
       attr[0].val.clusterDim.z = 1;
       cfg.attrs = attr;
@@ -409,7 +440,47 @@ template <typename T> struct NufftOp : Op {
   }
 
   int chi_slots() const override { return interp_blocks(); }
-  int tsv_slots() const override { return cdiv(nx, rpc); }
+  int max_chi_slots() const override { return std::max(1, cdiv(mmax, 8)); }
+  int tsv_slots() const override { return nx; }  // row-pass CTAs at rows_per_cta = 1
+
+  LaunchShapes shapes() const override {
+    LaunchShapes sh;
+    sh.interp_ppw = shared ? ippw : 0;
+    sh.spread_cluster = shared ? spread_cs : 0;
+    sh.rows_per_cta = rpc;
+    sh.cols_per_cta = cpc;
+    return sh;
+  }
+
+  void set_shapes(const LaunchShapes& sh) override {
+    auto rows_smem = [&](int r) { return (size_t)2 * r * (ny + 1) * sizeof(cplx<T>); };
+    auto cols_smem = [&](int cc) { return (size_t)2 * cc * (2 * nx + 1) * sizeof(cplx<T>); };
+    if (shared && sh.interp_ppw && (sh.interp_ppw < 1 || sh.interp_ppw > kMaxInterpPpw))
+      throw Error(MFISTA_ERR_ARG, "interp_ppw must be 1..32");
+    if (shared && sh.spread_cluster && (sh.spread_cluster < 1 || sh.spread_cluster > 16))
+      throw Error(MFISTA_ERR_ARG, "spread_cluster must be 1..16");
+    if (sh.rows_per_cta && (sh.rows_per_cta < 1 || sh.rows_per_cta > nx || rows_smem(sh.rows_per_cta) > 227 * 1024))
+      throw Error(MFISTA_ERR_ARG, "rows_per_cta out of range");
+    if (sh.cols_per_cta &&
+        (sh.cols_per_cta < 1 || sh.cols_per_cta > ny + 1 || cols_smem(sh.cols_per_cta) > 227 * 1024))
+      throw Error(MFISTA_ERR_ARG, "cols_per_cta out of range");
+    if (shared && sh.interp_ppw) {
+      ippw = sh.interp_ppw;
+      if (exact) exact->ippw = ippw;  // same chi^2 partial slots for forward_exact
+    }
+    if (shared && sh.spread_cluster) spread_cs = sh.spread_cluster;
+    if (sh.rows_per_cta) {
+      rpc = sh.rows_per_cta;
+      smem_rows = rows_smem(rpc);
+      set_smem(k_nufft_rows_fwd<T>, smem_rows);
+      set_smem(k_nufft_rows_inv<T>, smem_rows);
+    }
+    if (sh.cols_per_cta) {
+      cpc = sh.cols_per_cta;
+      smem_cols = cols_smem(cpc);
+      set_smem(k_nufft_cols<T>, smem_cols);
+    }
+  }
   double fscale() const override { return 0.5; }
   int launches_forward() const override { return 3; }
   int launches_adjoint() const override { return 3; }
@@ -550,6 +621,90 @@ template <typename T> struct FftVarOp : Op {
 // ---------------------------------------------------------------------------
 // dense DFT operator (FP64)
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// tensor-core split-BF16 GEMM launcher (tc::k_gemm_bf16x3)
+// ---------------------------------------------------------------------------
+inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  });
+  if (!fn) throw Error(MFISTA_ERR_CUDA, "the driver does not provide cuTensorMapEncodeTiled");
+  return fn;
+}
+
+// TMA map of a K-major BF16 plane [rows][kpad]: boxes of kTK x box_rows
+// elements with the 128-byte swizzle the MMA descriptors expect
+inline CUtensorMap bf16_tile_map(const void* base, int rows, int kpad, int box_rows) {
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (kpad % tc::kTK) || (rows % box_rows))
+    throw Error(MFISTA_ERR_ARG, "tensor-core operand not tiled");
+  CUtensorMap m;
+  cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)kpad * 2};
+  cuuint32_t box[2] = {(cuuint32_t)tc::kTK, (cuuint32_t)box_rows};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
+                                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(MFISTA_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return m;
+}
+
+// P[s][b][r] = sum_{k in split s} Amat[r][k] X[b][k] over K-major BF16 planes
+struct TcGemm {
+  int rows = 0, kpad = 0, bpad = 0, nsplit = 1, kblocks = 0, kblocks_all = 0;
+  CUtensorMap ahi{}, alo{}, xhi{}, xlo{};
+  DevMem part;  // [nsplit][bpad][rows] FP32
+  int* err = nullptr;
+
+  // split K so that the tiles cover the GPU's SMs about once (one CTA per SM)
+  void init(const void* a_hi, const void* a_lo, int rows_, int kpad_, const void* x_hi, const void* x_lo, int bpad_,
+            int* err_) {
+    rows = rows_;
+    kpad = kpad_;
+    bpad = bpad_;
+    err = err_;
+    kblocks_all = kpad / tc::kTK;
+    int dev = 0, sms = 148;
+    MF_CK(cudaGetDevice(&dev));
+    MF_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int tiles = (rows / tc::kTM) * (bpad / tc::kTN);
+    nsplit = std::max(1, std::min(kblocks_all, sms / std::max(tiles, 1)));
+    kblocks = cdiv(kblocks_all, nsplit);
+    nsplit = cdiv(kblocks_all, kblocks);  // no empty split
+    ahi = bf16_tile_map(a_hi, rows, kpad, tc::kTM);
+    alo = bf16_tile_map(a_lo, rows, kpad, tc::kTM);
+    xhi = bf16_tile_map(x_hi, bpad, kpad, tc::kTN);
+    xlo = bf16_tile_map(x_lo, bpad, kpad, tc::kTN);
+    part.alloc(sizeof(float) * (size_t)nsplit * bpad * rows);
+    MF_CK(cudaMemset(part.p, 0, part.bytes));
+    set_smem(tc::k_gemm_bf16x3, tc::kSmemBytes);
+  }
+
+  void launch(cudaStream_t s, const ProbState* st, int gate, int B) {
+    tc::TcArgs a{part.as<float>(), rows, bpad, kblocks, kblocks_all, err};
+    tc::k_gemm_bf16x3<<<dim3(rows / tc::kTM, nsplit, bpad / tc::kTN), 128, tc::kSmemBytes, s>>>(ahi, alo, xhi, xlo,
+                                                                                               a, st, gate, B);
+    MF_LAUNCH_CK();
+  }
+
+  // algorithmic bytes of one launch: both A planes, both X planes, partials
+  double bytes() const {
+    return 4.0 * rows * kpad + 4.0 * bpad * kpad + 4.0 * nsplit * bpad * rows;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// DFT operator: FP64 (GEMV for one problem, register-blocked GEMM for a
+// batch), or the split-BF16 tensor-core GEMMs with FP64 defect correction
+// ---------------------------------------------------------------------------
 struct DftOp : Op {
   Ctx& c;
   DftGeom g{};
@@ -557,9 +712,16 @@ struct DftOp : Op {
   int B;
   bool gemm = false;     // batched problems: GEMMs instead of per-problem GEMVs
   int mchunk = 0, nmchunk = 0;
+  // split-BF16 form
+  bool tcm = false;
+  int mrow = 0, nk = 0, nrow = 0, mk = 0, bpad = 0;
+  DevMem rm_hi, rm_lo, cm_hi, cm_lo, xv_hi, xv_lo, xr_hi, xr_lo, d_axa, d_ra, d_ga, d_err;
+  TcGemm fwd, adj;
 
-  DftOp(Ctx& ctx, const double* A, const double* y, int M, int N) : c(ctx) {
+  DftOp(Ctx& ctx, const double* A, const double* y, int M, int N, int precision = MFISTA_FP64) : c(ctx) {
     B = ctx.B;
+    tcm = precision == MFISTA_BF16X3;
+    if (!tcm && precision != MFISTA_FP64) throw Error(MFISTA_ERR_ARG, "the DFT operator runs in FP64 or BF16X3");
     d_A.upload(A, (size_t)M * N);
     d_y.upload(y, M);
     g.A = d_A.as<double>();
@@ -568,7 +730,7 @@ struct DftOp : Op {
     g.N = N;
     g.chunk = 64;
     g.nchunk = cdiv(N, g.chunk);
-    gemm = B > 1;
+    gemm = B > 1 || tcm;  // the anchors of the split-BF16 form use the FP64 GEMMs
     if (gemm) {  // split-K so that the tiles fill the GPU
       g.chunk = std::max(kGK, cdiv(cdiv(N, 4), kGK) * kGK);
       g.nchunk = cdiv(N, g.chunk);
@@ -580,9 +742,47 @@ struct DftOp : Op {
     d_resid.alloc(sizeof(double) * (size_t)B * std::max(M, 1));
     g.az_part = d_part.as<double>();
     g.resid = d_resid.as<double>();
+    if (tcm) setup_tc(M, N);
   }
 
-  void forward(cudaStream_t s, const double* src, int gate, int qchi, bool store) override {
+  void setup_tc(int M, int N) {
+    mrow = cdiv(M, tc::kTM) * tc::kTM;
+    nk = cdiv(N, tc::kTK) * tc::kTK;
+    nrow = cdiv(N, tc::kTM) * tc::kTM;
+    mk = cdiv(M, tc::kTK) * tc::kTK;
+    bpad = cdiv(B, tc::kTN) * tc::kTN;
+    const size_t h = 2;  // bytes per BF16
+    rm_hi.alloc(h * mrow * nk);
+    rm_lo.alloc(h * mrow * nk);
+    cm_hi.alloc(h * nrow * mk);
+    cm_lo.alloc(h * nrow * mk);
+    k_split_matrix_launch(M, N);
+    xv_hi.alloc(h * bpad * nk);
+    xv_lo.alloc(h * bpad * nk);
+    xr_hi.alloc(h * bpad * mk);
+    xr_lo.alloc(h * bpad * mk);
+    for (DevMem* d : {&xv_hi, &xv_lo, &xr_hi, &xr_lo}) MF_CK(cudaMemset(d->p, 0, d->bytes));
+    d_axa.alloc(sizeof(double) * (size_t)B * M);
+    d_ra.alloc(sizeof(double) * (size_t)B * M);
+    d_ga.alloc(sizeof(double) * (size_t)B * N);
+    for (DevMem* d : {&d_axa, &d_ra, &d_ga}) MF_CK(cudaMemset(d->p, 0, d->bytes));
+    d_err.alloc(sizeof(int));
+    MF_CK(cudaMemset(d_err.p, 0, sizeof(int)));
+    fwd.init(rm_hi.p, rm_lo.p, mrow, nk, xv_hi.p, xv_lo.p, bpad, d_err.as<int>());
+    adj.init(cm_hi.p, cm_lo.p, nrow, mk, xr_hi.p, xr_lo.p, bpad, d_err.as<int>());
+    MF_CK(cudaDeviceSynchronize());
+  }
+
+  void k_split_matrix_launch(int M, int N) {
+    dim3 grid(cdiv(std::max(mrow, mk), 32), cdiv(std::max(nrow, nk), 32));
+    tc::k_split_matrix<<<grid, 256>>>(g.A, M, N, mrow, nk, nrow, mk, rm_hi.as<__nv_bfloat16>(),
+                                      rm_lo.as<__nv_bfloat16>(), cm_hi.as<__nv_bfloat16>(),
+                                      cm_lo.as<__nv_bfloat16>());
+    MF_LAUNCH_CK();
+  }
+
+  // FP64 A z -> residual (and chi^2 partials)
+  void forward_fp64(cudaStream_t s, const double* src, int gate, int qchi, bool store) {
     if (gemm)
       k_dft_az_gemm<<<dim3(cdiv(g.M, kGT), g.nchunk, cdiv(B, kGT)), 256, 0, s>>>(g, src, c.xstride, c.st, gate, B);
     else
@@ -593,7 +793,35 @@ struct DftOp : Op {
     MF_LAUNCH_CK();
   }
 
+  void forward(cudaStream_t s, const double* src, int gate, int qchi, bool store) override {
+    if (!tcm) {
+      forward_fp64(s, src, gate, qchi, store);
+      return;
+    }
+    tc::k_split_vectors<<<dim3(cdiv(nk, 256), bpad), 256, 0, s>>>(src, c.xstride, c.xa, c.xstride, g.N, nk, B, c.st,
+                                                                   gate, xv_hi.as<__nv_bfloat16>(),
+                                                                   xv_lo.as<__nv_bfloat16>());
+    MF_LAUNCH_CK();
+    fwd.launch(s, c.st, gate, B);
+    k_dft_tc_resid<<<dim3(std::max(1, cdiv(g.M, 256)), B), 256, 0, s>>>(fwd.part.as<float>(), fwd.nsplit, bpad, mrow,
+                                                                        d_axa.as<double>(), g, c.st, gate, c.part,
+                                                                        qchi, store ? 1 : 0);
+    MF_LAUNCH_CK();
+  }
+
   void adjoint(cudaStream_t s, const double* z_tsv, int qtsv) override {
+    if (tcm) {
+      tc::k_split_vectors<<<dim3(cdiv(mk, 256), bpad), 256, 0, s>>>(g.resid, g.M, d_ra.as<double>(), g.M, g.M, mk, B,
+                                                                     c.st, kGateGrad, xr_hi.as<__nv_bfloat16>(),
+                                                                     xr_lo.as<__nv_bfloat16>());
+      MF_LAUNCH_CK();
+      adj.launch(s, c.st, kGateGrad, B);
+      k_dft_tc_atr_finish<<<dim3(cdiv(g.N, 256), B), 256, 0, s>>>(adj.part.as<float>(), adj.nsplit, bpad, nrow,
+                                                                   d_ga.as<double>(), g.N, c.dfdx, c.xstride, z_tsv,
+                                                                   c.prm, c.tsvNX, c.tsvNY, c.st, kGateGrad);
+      MF_LAUNCH_CK();
+      return;
+    }
     if (gemm) {
       k_dft_atr_gemm<<<dim3(cdiv(g.N, kGT), nmchunk, cdiv(B, kGT)), 256, 0, s>>>(g, d_atr.as<double>(), mchunk,
                                                                                  nmchunk, c.st, kGateGrad, B);
@@ -608,11 +836,75 @@ struct DftOp : Op {
     MF_LAUNCH_CK();
   }
 
+  // FP64 A^T r over a residual buffer (FP64 GEMM; no TSV term)
+  void atr_fp64(cudaStream_t s, const double* resid, double* out, long ostride, int gate) {
+    DftGeom gg = g;
+    gg.resid = const_cast<double*>(resid);
+    k_dft_atr_gemm<<<dim3(cdiv(g.N, kGT), nmchunk, cdiv(B, kGT)), 256, 0, s>>>(gg, d_atr.as<double>(), mchunk,
+                                                                               nmchunk, c.st, gate, B);
+    MF_LAUNCH_CK();
+    k_dft_atr_finish<<<dim3(cdiv(g.N, 256), B), 256, 0, s>>>(gg, d_atr.as<double>(), nmchunk, out, ostride, nullptr,
+                                                             c.prm, c.tsvNX, c.tsvNY, c.st, gate);
+    MF_LAUNCH_CK();
+  }
+
+  bool corrected() const override { return tcm; }
+  int launches_refresh() const override { return tcm ? 4 : 0; }
+
+  // FP64 anchor terms: ax_a = A x_a, r_a = y - ax_a, g_a = A^T r_a
+  void refresh_anchor(cudaStream_t s, int gate) override {
+    if (!tcm) return;
+    k_dft_az_gemm<<<dim3(cdiv(g.M, kGT), g.nchunk, cdiv(B, kGT)), 256, 0, s>>>(g, c.xa, c.xstride, c.st, gate, B);
+    MF_LAUNCH_CK();
+    k_dft_anchor<<<dim3(std::max(1, cdiv(g.M, 256)), B), 256, 0, s>>>(g, c.st, gate, d_axa.as<double>(),
+                                                                      d_ra.as<double>());
+    MF_LAUNCH_CK();
+    atr_fp64(s, d_ra.as<double>(), d_ga.as<double>(), g.N, gate);
+  }
+
+  void forward_exact(cudaStream_t s, const double* src, int gate, int qchi, bool store) override {
+    forward_fp64(s, src, gate, qchi, store);
+  }
+
+  int device_error() override {
+    if (!tcm) return 0;
+    int e = 0;
+    MF_CK(cudaMemcpy(&e, d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    return e;
+  }
+
+  // 0: A z GEMM, 1: A^T r GEMM (the split-BF16 ones when in that form)
+  double launch_single(cudaStream_t s, int kernel) override {
+    if (kernel == 0) {
+      if (tcm) {
+        fwd.launch(s, c.st, kGateAll, B);
+        return fwd.bytes();
+      }
+      if (!gemm) return -1;
+      k_dft_az_gemm<<<dim3(cdiv(g.M, kGT), g.nchunk, cdiv(B, kGT)), 256, 0, s>>>(g, c.z, c.xstride, c.st, kGateAll,
+                                                                                 B);
+      MF_LAUNCH_CK();
+      return 8.0 * g.M * g.N + 8.0 * B * g.N + 8.0 * B * g.nchunk * g.M;
+    }
+    if (kernel == 1) {
+      if (tcm) {
+        adj.launch(s, c.st, kGateAll, B);
+        return adj.bytes();
+      }
+      if (!gemm) return -1;
+      k_dft_atr_gemm<<<dim3(cdiv(g.N, kGT), nmchunk, cdiv(B, kGT)), 256, 0, s>>>(g, d_atr.as<double>(), mchunk,
+                                                                                 nmchunk, c.st, kGateAll, B);
+      MF_LAUNCH_CK();
+      return 8.0 * g.M * g.N + 8.0 * B * g.M + 8.0 * B * nmchunk * g.N;
+    }
+    return -1;
+  }
+
   int chi_slots() const override { return std::max(1, cdiv(g.M, 256)); }
   int tsv_slots() const override { return cdiv(g.N, 8); }
   double fscale() const override { return 0.5; }
-  int launches_forward() const override { return 2; }
-  int launches_adjoint() const override { return gemm ? 2 : 1; }
+  int launches_forward() const override { return tcm ? 3 : 2; }
+  int launches_adjoint() const override { return tcm ? 3 : (gemm ? 2 : 1); }
 };
 
 // ---------------------------------------------------------------------------
@@ -700,7 +992,8 @@ struct Solver {
   int img_blocks() const { return cdiv(ctx.N, 256); }
 
   void finish_setup() {
-    int slots = std::max({op->chi_slots(), op->tsv_slots(), img_blocks(), 1});
+    // capacity for every launch shape, so that set_shapes/tune never regrow it
+    int slots = std::max({op->max_chi_slots(), op->tsv_slots(), img_blocks(), 1});
     d_part.alloc(sizeof(double) * (size_t)kNumQ * ctx.B * slots);
     MF_CK(cudaMemset(d_part.p, 0, d_part.bytes));
     ctx.part.p = d_part.as<double>();
@@ -738,7 +1031,7 @@ struct Solver {
 
   template <typename K> void prep_fgp_kernel(K kern, int cs, size_t smem) {
     if (cs > 8) MF_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    if (smem) MF_CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (smem) set_smem(kern, smem);
   }
 
   // Picks the FGP cluster shape: slabs in shared memory with 8 or 16 CTAs
@@ -860,6 +1153,79 @@ struct Solver {
     launch_control(s, kCtrlStep, h, set_handle);
     k_momentum<<<ig, 256, 0, s>>>(ctx.x, ctx.z, ctx.xnew, dm, ctx.st);
     MF_LAUNCH_CK();
+  }
+
+  void drop_graphs() {
+    if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+    if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+    if (body_exec) { cudaGraphExecDestroy(body_exec); body_exec = nullptr; }
+    if (body_graph) { cudaGraphDestroy(body_graph); body_graph = nullptr; }
+  }
+
+  // new operator launch shapes; the solve graph is captured again
+  void apply_shapes(const LaunchShapes& sh) {
+    MF_CK(cudaStreamSynchronize(stream));
+    op->set_shapes(sh);
+    drop_graphs();
+    const char* hl = getenv("MFISTA_HOST_LOOP");
+    host_loop = hl && hl[0] == '1';
+    build_graph();
+  }
+
+  // Autotuner: times each operator kernel alone (profile_kernel, every
+  // problem active) over its candidate shapes, one knob at a time with the
+  // others at their current choice, keeps the fastest and captures the
+  // graph again.  ms_out[k]: best time (ms per launch) for knob k.
+  LaunchShapes tune(int reps, double ms_out[4]) {
+    LaunchShapes cur = op->shapes();
+    // knob -> kernels timed (profile_kernel ids) and candidates
+    struct Knob { int LaunchShapes::*field; std::vector<int> kernels; std::vector<int> cand; };
+    std::vector<Knob> knobs = {
+        {&LaunchShapes::interp_ppw, {0}, {1, 2, 4, 8, 16}},
+        {&LaunchShapes::spread_cluster, {1}, {1, 2, 4, 8, 16}},
+        {&LaunchShapes::rows_per_cta, {2, 5}, {1, 2, 4, 8, 16}},
+        {&LaunchShapes::cols_per_cta, {3, 4}, {1, 2, 4, 8, 16}},
+    };
+    for (size_t k = 0; k < knobs.size(); ++k) {
+      ms_out[k] = 0;
+      Knob& kb = knobs[k];
+      if (cur.*(kb.field) == 0) continue;  // not used by this operator
+      double best = 1e300;
+      int best_v = cur.*(kb.field);
+      for (int v : kb.cand) {
+        LaunchShapes tr = cur;
+        tr.*(kb.field) = v;
+        try {
+          op->set_shapes(tr);
+        } catch (const Error&) {
+          continue;  // shape not possible for this problem size
+        }
+        if (kb.field == &LaunchShapes::spread_cluster && !spread_cluster_fits(v)) continue;
+        double t = 0;
+        for (int kern : kb.kernels) {
+          double ms = 0, by = 0;
+          profile_kernel(kern, 1, ms, by);  // warm
+          profile_kernel(kern, reps, ms, by);
+          t += ms;
+        }
+        if (t < best) {
+          best = t;
+          best_v = v;
+        }
+      }
+      cur.*(kb.field) = best_v;
+      op->set_shapes(cur);
+      ms_out[k] = best;
+    }
+    apply_shapes(cur);
+    return cur;
+  }
+
+  // can a cluster of `cs` spreading CTAs be resident on this GPU?
+  bool spread_cluster_fits(int cs) {
+    if (precision == MFISTA_FP32)
+      return max_clusters(k_nufft_spread_shared<float>, cs, sizeof(cplx<float>) * SharedChunk<float>::kSpread * 256) > 0;
+    return max_clusters(k_nufft_spread_shared<double>, cs, sizeof(cplx<double>) * SharedChunk<double>::kSpread * 256) > 0;
   }
 
   void build_graph() {

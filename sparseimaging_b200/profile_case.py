@@ -35,6 +35,8 @@ def main():
                     help="max|A^H W^2 y| (skips its GPU computation when given)")
     ap.add_argument("--lip", type=float, default=0.0,
                     help="Lipschitz estimate for cinit (skips the power iteration when given)")
+    ap.add_argument("--shapes", default="",
+                    help="launch shapes interp_ppw,spread_cluster,rows_per_cta,cols_per_cta (0 keeps a default)")
     a = ap.parse_args()
     os.environ.setdefault("MFISTA_QUIET", "1")
     import sparseimaging_b200 as si
@@ -52,8 +54,11 @@ def main():
     probs = [dict(lambda_l1=float(l1), lambda_tsv=float(lt), cinit=lip, maxiter=a.iters, nonneg_flag=1)
              for l1, lt in grid]
     plan = si.Plan(p.u_dx, p.v_dy, p.vis_r, p.vis_i, p.vis_std, nx, nx, len(probs), precision=a.precision)
+    if a.shapes:
+        vals = [int(v) for v in a.shapes.split(",")]
+        plan.set_shapes(**dict(zip(si.Plan.SHAPE_KEYS, vals)))
     plan.set_problems(probs, 0.0)
-    out = {"case": a.case, "precision": a.precision, "problems": len(probs), "M": p.m}
+    out = {"case": a.case, "precision": a.precision, "problems": len(probs), "M": p.m, "shapes": plan.shapes()}
     if a.kernel >= 0:
         ms, by = plan.profile(a.kernel, a.reps)
         out.update(kernel=a.kernel, ms_per_launch=ms, bytes_per_launch=by, gbs=by / ms / 1e6)

@@ -31,8 +31,10 @@ def res_dict(arr):
 
 
 def rel(a, b):
-    a = np.asarray(a, np.float64)
-    b = np.asarray(b, np.float64)
+    """Relative L2 error of a against b (complex inputs compared as complex)."""
+    cplx = np.iscomplexobj(a) or np.iscomplexobj(b)
+    a = np.asarray(a, np.complex128 if cplx else np.float64)
+    b = np.asarray(b, np.complex128 if cplx else np.float64)
     nb = np.linalg.norm(b)
     return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
 
