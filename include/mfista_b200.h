@@ -114,11 +114,18 @@ int mfista_set_fgp_iter(int n);
 
 /* Arithmetic of the operators (spread/interp/FFT/stencils).  The objective,
  * reductions, backtracking test and FISTA sequence are FP64 in both. */
-enum mfista_precision { MFISTA_FP64 = 64, MFISTA_FP32 = 32, MFISTA_BF16X3 = 3 };
-/* MFISTA_BF16X3 (DFT operator only): A z and A^T r on the tensor cores as
- * three BF16 products of split operands (hi*hi + hi*lo + lo*hi) with FP32
- * accumulation, applied to the departure from an FP64 anchor that is
- * refreshed every 32 outer iterations, so results keep FP64 accuracy. */
+enum mfista_precision {
+  MFISTA_FP64 = 64,
+  MFISTA_FP32 = 32,
+  MFISTA_BF16X3 = 3,
+  MFISTA_BF16X6 = 6
+};
+/* MFISTA_BF16X3 / MFISTA_BF16X6 (DFT operator only): A z and A^T r on the
+ * tensor cores from BF16 split operands with FP32 accumulation: two planes
+ * each and three products (hi*hi + hi*lo + lo*hi, ~2^-16 relative), or
+ * three planes each and six products (~2^-24, FP32-like).  The solver applies
+ * them to the departure from an FP64 anchor refreshed every 8 (BF16X3) or 32
+ * (BF16X6) outer iterations. */
 
 /* Per-problem parameters of a batched solve. */
 struct mfista_problem {
@@ -243,10 +250,17 @@ int mfista_nufft_forward_noalloc(const double *u_dx, const double *v_dy, int M, 
  * :253-278, batched): A is column-major M x N;
  *   transpose = 0: out[b][m] = sum_n A[m + n M] X[b][n]   (X [B][N], out [B][M])
  *   transpose = 1: out[b][n] = sum_m A[m + n M] X[b][m]   (X [B][M], out [B][N])
- * precision MFISTA_FP64, or MFISTA_BF16X3 for the tensor-core split-BF16
- * GEMM alone (no anchor: ~1e-5 relative error). */
+ * precision MFISTA_FP64, or MFISTA_BF16X3 / MFISTA_BF16X6 for the
+ * tensor-core split-BF16 GEMM alone (no anchor: ~1e-5 / ~1e-7 relative
+ * error). */
 int mfista_dft_apply(const double *A, int M, int N, const double *X, int B, int transpose, int precision,
                      double *out);
+
+/* Times one DFT operator kernel alone for a batch of B problems sharing A
+ * (as mfista_plan_profile): kernel 0 = the A z GEMM, 1 = the A^T r GEMM, in
+ * the given precision (MFISTA_FP64 needs B > 1: the batched GEMMs). */
+int mfista_dft_profile(const double *A, int M, int N, int B, int precision, int kernel, int reps,
+                       double *ms_per_launch, double *bytes_per_launch);
 
 /* FGP TV proximal map alone (FGP_L1_box / FGP_nonneg_box,
  * c/mfista_TV_lib.c:189-384) on an NX x NY view: x_out = prox(b). */

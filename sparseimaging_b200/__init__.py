@@ -23,10 +23,12 @@ __all__ = ["RESULT", "Problem", "MfistaError", "lib", "mfista_imaging_core_nufft
            "mfista_imaging_core_fft", "mfista_imaging_core_dft", "imaging_core_nufft",
            "imaging_core_fft", "imaging_core_dft", "nufft_batch", "dft_batch", "Plan", "nufft_forward",
            "nufft_adjoint", "fgp_prox", "nufft_lipschitz", "last_status", "last_error", "set_fgp_iter", "set_device",
-           "FP64", "FP32"]
+           "dft_apply", "dft_profile", "FP64", "FP32", "BF16X3", "BF16X6"]
 
 FP64 = 64
 FP32 = 32
+BF16X3 = 3  # DFT only: tensor-core split-BF16 products (2 planes, 3 products) with FP64 anchor correction
+BF16X6 = 6  # DFT only: 3 planes, 6 products (~FP32 accuracy) with FP64 anchor correction
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -125,6 +127,10 @@ def lib():
         L.mfista_plan_set_shapes.argtypes = [C.c_void_p, _i4]
         L.mfista_plan_tune.restype = C.c_int
         L.mfista_plan_tune.argtypes = [C.c_void_p, C.c_int, _i4, _dp]
+        L.mfista_dft_apply.restype = C.c_int
+        L.mfista_dft_apply.argtypes = [_dp, C.c_int, C.c_int, _dp, C.c_int, C.c_int, C.c_int, _dp]
+        L.mfista_dft_profile.restype = C.c_int
+        L.mfista_dft_profile.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]
         L.mfista_plan_destroy.restype = None
         L.mfista_plan_destroy.argtypes = [C.c_void_p]
         L.mfista_nufft_forward.restype = C.c_int
@@ -304,8 +310,11 @@ def nufft_batch(u_dx, v_dy, vis_r, vis_i, vis_std, nx, ny, problems, eps, precis
     return xo.reshape(B, n), [r.as_dict() for r in res]
 
 
-def dft_batch(y, A, nx, ny, problems, eps, xinit=None, fgp_iter=100):
-    """Solves len(problems) DFT problems sharing A (logical (M, N)) and y."""
+def dft_batch(y, A, nx, ny, problems, eps, xinit=None, fgp_iter=100, precision=None):
+    """Solves len(problems) DFT problems sharing A (logical (M, N)) and y;
+    precision FP64 (default) or BF16X3 (tensor-core split-BF16 GEMMs with
+    FP64 anchor correction)."""
+    precision = FP64 if precision is None else precision
     A = np.asarray(A, np.float64)
     m, n = A.shape
     Af = np.asfortranarray(A)
@@ -315,9 +324,39 @@ def dft_batch(y, A, nx, ny, problems, eps, xinit=None, fgp_iter=100):
     xo = np.zeros(B * n)
     res = (RESULT * B)()
     st = lib().mfista_dft_batch(_p(yy), Af.ctypes.data_as(_dp), m, n, nx, ny, B, _problems(problems), eps,
-                                FP64, fgp_iter, _p(xi), _p(xo), res)
+                                precision, fgp_iter, _p(xi), _p(xo), res)
     _check(st)
     return xo.reshape(B, n), [r.as_dict() for r in res]
+
+
+def dft_apply(A, X, transpose=False, precision=None):
+    """A @ x_b (or A.T @ x_b) for every row x_b of X, on the GPU; A is (M, N).
+    precision FP64 or BF16X3 (the tensor-core split-BF16 GEMM alone)."""
+    precision = FP64 if precision is None else precision
+    A = np.asarray(A, np.float64)
+    m, n = A.shape
+    Af = np.asfortranarray(A)
+    X = np.ascontiguousarray(np.atleast_2d(X), np.float64)
+    B = X.shape[0]
+    if X.shape[1] != (m if transpose else n):
+        raise ValueError("X has the wrong length for this product")
+    out = np.zeros((B, n if transpose else m))
+    _check(lib().mfista_dft_apply(Af.ctypes.data_as(_dp), m, n, _p(X), B, int(bool(transpose)), precision,
+                                  _p(out)))
+    return out
+
+
+def dft_profile(A, B, kernel, precision=None, reps=20):
+    """(ms per launch, algorithmic bytes per launch) of the batched DFT GEMM
+    `kernel` (0: A z, 1: A^T r) for B problems sharing A (M, N)."""
+    precision = FP64 if precision is None else precision
+    A = np.asarray(A, np.float64)
+    m, n = A.shape
+    Af = np.asfortranarray(A)
+    ms, by = C.c_double(0), C.c_double(0)
+    _check(lib().mfista_dft_profile(Af.ctypes.data_as(_dp), m, n, B, precision, kernel, reps, C.byref(ms),
+                                    C.byref(by)))
+    return ms.value, by.value
 
 
 class Plan:

@@ -104,12 +104,25 @@ namespace mf {
 constexpr int kGT = 64;   // tile edge (rows and problems)
 constexpr int kGK = 16;   // K step staged in shared memory
 
+// does any problem b0 .. b0 + kGT - 1 pass the gate?  (uniform over the CTA)
+__device__ __forceinline__ bool tile_active(const ProbState* __restrict__ st, int gate, int b0, int B) {
+  __shared__ int s_any;
+  if (threadIdx.x == 0) {
+    int any = 0;
+    for (int i = 0; i < kGT && b0 + i < B; ++i) any |= gate_ok(st[b0 + i], gate) ? 1 : 0;
+    s_any = any;
+  }
+  __syncthreads();
+  return s_any != 0;
+}
+
 // az_part[b][chunk][m] = sum_{n in chunk} A[m + n M] z_b[n]
 __global__ void __launch_bounds__(256) k_dft_az_gemm(DftGeom g, const double* __restrict__ zall, long xstride,
                                                      const ProbState* __restrict__ st, int gate, int B) {
   __shared__ double sA[kGK][kGT + 1];
   __shared__ double sZ[kGK][kGT + 1];
   const int m0 = blockIdx.x * kGT, b0 = blockIdx.z * kGT, c = blockIdx.y;
+  if (!tile_active(st, gate, b0, B)) return;  // no problem of this tile: skip reading A
   const int n0 = c * g.chunk, n1 = min(g.N, n0 + g.chunk);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16 threads, 4 x 4 outputs each
   double acc[4][4];
@@ -159,6 +172,7 @@ __global__ void __launch_bounds__(256) k_dft_atr_gemm(DftGeom g, double* __restr
   __shared__ double sA[kGK][kGT + 1];
   __shared__ double sR[kGK][kGT + 1];
   const int nn0 = blockIdx.x * kGT, b0 = blockIdx.z * kGT, c = blockIdx.y;
+  if (!tile_active(st, gate, b0, B)) return;
   const int ms = c * mchunk, me = min(g.M, ms + mchunk);
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   double acc[4][4];

@@ -3,15 +3,18 @@
 //
 //   P[s][b][r] = sum_{k in K-split s} Amat[r][k] * X[b][k]
 //
-// with both operands K-major in BF16 "split" form: Amat = Ahi + Alo and
-// X = Xhi + Xlo, each plane BF16, and
+// with both operands K-major in BF16 "split" form, NP planes each
+// (Amat = A0 + A1 [+ A2], every plane BF16, the next plane the rounding
+// residual of the previous ones), and
 //
-//   Amat X  ~  Ahi Xhi + Ahi Xlo + Alo Xhi            (3 MMAs per K step)
+//   NP = 2:  Amat X ~ A0 X0 + A0 X1 + A1 X0                       (3 MMAs)
+//   NP = 3:  Amat X ~ A0 X0 + A0 X1 + A1 X0 + A0 X2 + A1 X1 + A2 X0 (6 MMAs)
 //
-// accumulated in FP32 in tensor memory.  The dropped Alo Xlo term and the
-// rounding of the planes leave ~2^-16 relative error per product; callers
-// apply it only to the difference between an iterate and an FP64 anchor
-// (defect correction), so the solve keeps FP64 accuracy.
+// per K step, accumulated in FP32 in tensor memory.  The dropped terms and
+// the rounding of the planes leave ~2^-16 (NP = 2) or ~2^-24 (NP = 3)
+// relative error per product; callers apply it only to the difference
+// between an iterate and an FP64 anchor (defect correction), so the solve
+// keeps FP64 accuracy.
 //
 // One CTA computes a 128-row x 64-problem tile over one K split:
 //   * one thread issues TMA tile loads (128-byte swizzle) into a 4-stage
@@ -38,11 +41,21 @@ namespace tc {
 constexpr int kTM = 128;                            // tile rows (MMA M)
 constexpr int kTN = 64;                             // tile problems (MMA N)
 constexpr int kTK = 64;                             // K per stage: 128 B of BF16
-constexpr int kStages = 4;
-constexpr int kATile = kTM * kTK * 2;               // 16 KB
-constexpr int kXTile = kTN * kTK * 2;               // 8 KB
-constexpr int kStageBytes = 2 * kATile + 2 * kXTile;
-constexpr int kSmemBytes = kStages * kStageBytes + 1024;  // + alignment slack
+constexpr int kATile = kTM * kTK * 2;               // 16 KB per plane
+constexpr int kXTile = kTN * kTK * 2;               // 8 KB per plane
+
+// shared-memory ring of a kernel with NP planes per operand
+template <int NP> struct Ring {
+  static constexpr int kStageBytes = NP * (kATile + kXTile);
+  static constexpr int kStages = NP == 2 ? 4 : 3;
+  static constexpr int kSmemBytes = kStages * kStageBytes + 1024;  // + alignment slack
+};
+
+// TMA maps of the operand planes (plane p of A, of X)
+struct TcMaps {
+  CUtensorMap a[3];
+  CUtensorMap x[3];
+};
 constexpr uint32_t kTmemCols = 64;                  // FP32 accumulator: 128 lanes x 64 columns
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound on every wait
 
@@ -142,11 +155,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// grid (rows / kTM, nsplit, bpad / kTN), 128 threads, kSmemBytes dynamic smem
+// grid (rows / kTM, nsplit, bpad / kTN), 128 threads, Ring<NP>::kSmemBytes
+// dynamic shared memory
+template <int NP>
 __global__ void __launch_bounds__(128, 1)
-    k_gemm_bf16x3(const __grid_constant__ CUtensorMap tm_ahi, const __grid_constant__ CUtensorMap tm_alo,
-                  const __grid_constant__ CUtensorMap tm_xhi, const __grid_constant__ CUtensorMap tm_xlo, TcArgs g,
-                  const ProbState* __restrict__ st, int gate, int B) {
+    k_gemm_split_bf16(const __grid_constant__ TcMaps maps, TcArgs g, const ProbState* __restrict__ st, int gate,
+                      int B) {
+  constexpr int kStages = Ring<NP>::kStages;
+  constexpr int kStageBytes = Ring<NP>::kStageBytes;
   extern __shared__ unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t full[kStages], empty[kStages], accf;
   __shared__ uint32_t tmem_slot;
@@ -198,10 +214,10 @@ __global__ void __launch_bounds__(128, 1)
       unsigned char* sb = ring + s * kStageBytes;
       mbar_expect_tx(&full[s], kStageBytes);
       const int kx = (kb0 + kb) * kTK;
-      tma_load_2d(sb, &tm_ahi, kx, row0, &full[s]);
-      tma_load_2d(sb + kATile, &tm_alo, kx, row0, &full[s]);
-      tma_load_2d(sb + 2 * kATile, &tm_xhi, kx, b0, &full[s]);
-      tma_load_2d(sb + 2 * kATile + kXTile, &tm_xlo, kx, b0, &full[s]);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) tma_load_2d(sb + p * kATile, &maps.a[p], kx, row0, &full[s]);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) tma_load_2d(sb + NP * kATile + p * kXTile, &maps.x[p], kx, b0, &full[s]);
       issued = kb + 1;
     }
     if (failed) {  // let the copies already issued land before the CTA exits
@@ -209,7 +225,7 @@ __global__ void __launch_bounds__(128, 1)
         mbar_wait(&full[kb % kStages], (kb / kStages) & 1, kWaitNs);
     }
   } else if (warp == 1 && lane == 0) {
-    // MMA issuer
+    // MMA issuer: products A_i X_j with i + j < NP, lowest order first
     for (int kb = 0; kb < nk; ++kb) {
       const int s = kb % kStages;
       if (!mbar_wait(&full[s], (kb / kStages) & 1, kWaitNs)) {
@@ -218,14 +234,20 @@ __global__ void __launch_bounds__(128, 1)
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       unsigned char* sb = ring + s * kStageBytes;
-      const uint64_t ah = sw128_desc(sb), al = sw128_desc(sb + kATile);
-      const uint64_t xh = sw128_desc(sb + 2 * kATile), xl = sw128_desc(sb + 2 * kATile + kXTile);
+      uint64_t ad[NP], xd[NP];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        ad[p] = sw128_desc(sb + p * kATile);
+        xd[p] = sw128_desc(sb + NP * kATile + p * kXTile);
+      }
 #pragma unroll
       for (int j = 0; j < kTK / 16; ++j) {
         const uint64_t dk = (uint64_t)(j * 32) >> 4;  // 16 BF16 = 32 B further along K
-        umma_bf16(tmem, ah + dk, xh + dk, (kb > 0 || j > 0) ? 1u : 0u);
-        umma_bf16(tmem, ah + dk, xl + dk, 1u);
-        umma_bf16(tmem, al + dk, xh + dk, 1u);
+        umma_bf16(tmem, ad[0] + dk, xd[0] + dk, (kb > 0 || j > 0) ? 1u : 0u);
+#pragma unroll
+        for (int ord = 1; ord < NP; ++ord)
+#pragma unroll
+          for (int i = 0; i <= ord; ++i) umma_bf16(tmem, ad[i] + dk, xd[ord - i] + dk, 1u);
       }
       umma_commit(&empty[s]);  // the stage is free once these MMAs have read it
     }
@@ -255,6 +277,19 @@ __global__ void __launch_bounds__(128, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
+// plane p of the split of v: v = P0 + P1 [+ P2], each BF16
+template <int NP> __device__ __forceinline__ void split_value(double v, __nv_bfloat16 (&q)[NP]) {
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    q[p] = __double2bfloat16(v);
+    v -= (double)__bfloat162float(q[p]);
+  }
+}
+
+struct Planes {
+  __nv_bfloat16* p[3];
+};
+
 // BF16 split planes of a column-major FP64 matrix A (M x N, A[m + n M]):
 //   rm: [mrow][nk]  rows m, K = n contiguous  -- operand of A x
 //   cm: [nrow][mk]  rows n, K = m contiguous  -- operand of A^T r
@@ -262,9 +297,9 @@ __global__ void __launch_bounds__(128, 1)
 // zero).  32 x 32 tiles through shared memory so both layouts are written
 // with coalesced stores; grid (cdiv(max(mrow, mk), 32), cdiv(max(nrow, nk), 32)),
 // 256 threads.
+template <int NP>
 __global__ void k_split_matrix(const double* __restrict__ A, int M, int N, int mrow, int nk, int nrow, int mk,
-                               __nv_bfloat16* __restrict__ rm_hi, __nv_bfloat16* __restrict__ rm_lo,
-                               __nv_bfloat16* __restrict__ cm_hi, __nv_bfloat16* __restrict__ cm_lo) {
+                               Planes rm, Planes cm) {
   __shared__ double t[32][33];
   const int m0 = blockIdx.x * 32, n0 = blockIdx.y * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
@@ -276,19 +311,19 @@ __global__ void k_split_matrix(const double* __restrict__ A, int M, int N, int m
   for (int j = ty; j < 32; j += 8) {  // cm: row n, consecutive threads along m
     int n = n0 + j, m = m0 + tx;
     if (n < nrow && m < mk) {
-      double v = t[j][tx];
-      __nv_bfloat16 h = __double2bfloat16(v);
-      cm_hi[(size_t)n * mk + m] = h;
-      cm_lo[(size_t)n * mk + m] = __double2bfloat16(v - (double)__bfloat162float(h));
+      __nv_bfloat16 q[NP];
+      split_value<NP>(t[j][tx], q);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) cm.p[p][(size_t)n * mk + m] = q[p];
     }
   }
   for (int j = ty; j < 32; j += 8) {  // rm: row m, consecutive threads along n
     int m = m0 + j, n = n0 + tx;
     if (m < mrow && n < nk) {
-      double v = t[tx][j];
-      __nv_bfloat16 h = __double2bfloat16(v);
-      rm_hi[(size_t)m * nk + n] = h;
-      rm_lo[(size_t)m * nk + n] = __double2bfloat16(v - (double)__bfloat162float(h));
+      __nv_bfloat16 q[NP];
+      split_value<NP>(t[tx][j], q);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) rm.p[p][(size_t)m * nk + n] = q[p];
     }
   }
 }
@@ -296,9 +331,10 @@ __global__ void k_split_matrix(const double* __restrict__ A, int M, int N, int m
 // BF16 split planes of a batch of vectors, X[b][k] = src[b][k] - sub[b][k]
 // (sub may be null), K-major [bpad][kpad]; problems outside the gate or
 // beyond B, and the K padding, are zero
+template <int NP>
 __global__ void k_split_vectors(const double* __restrict__ src, long sstride, const double* __restrict__ sub,
                                 long substride, int K, int kpad, int B, const ProbState* __restrict__ st, int gate,
-                                __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+                                Planes x) {
   const int b = blockIdx.y;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= kpad) return;
@@ -307,9 +343,10 @@ __global__ void k_split_vectors(const double* __restrict__ src, long sstride, co
     v = src[(size_t)b * sstride + k];
     if (sub) v -= sub[(size_t)b * substride + k];
   }
-  __nv_bfloat16 h = __double2bfloat16(v);
-  hi[(size_t)b * kpad + k] = h;
-  lo[(size_t)b * kpad + k] = __double2bfloat16(v - (double)__bfloat162float(h));
+  __nv_bfloat16 q[NP];
+  split_value<NP>(v, q);
+#pragma unroll
+  for (int p = 0; p < NP; ++p) x.p[p][(size_t)b * kpad + k] = q[p];
 }
 
 }  // namespace tc

@@ -472,8 +472,8 @@ extern "C" int mfista_dft_batch(const double* y, const double* A, int M, int N, 
   set_ok();
   try {
     if (B < 1) throw Error(MFISTA_ERR_ARG, "B must be >= 1");
-    if (precision != MFISTA_FP64 && precision != MFISTA_BF16X3)
-      throw Error(MFISTA_ERR_ARG, "the batched DFT runs in FP64 or BF16X3");
+    if (precision != MFISTA_FP64 && precision != MFISTA_BF16X3 && precision != MFISTA_BF16X6)
+      throw Error(MFISTA_ERR_ARG, "the batched DFT runs in FP64, BF16X3 or BF16X6");
     int form = problems[0].lambda_tv != 0 ? kFormTV : kFormTSV;
     std::vector<ProbParams> prm(B);
     for (int b = 0; b < B; ++b) {
@@ -538,12 +538,12 @@ int nufft_apply(const double* u, const double* v, const double* wstd, int M, int
   memset(&st, 0, sizeof(st));
   st.active = 1;
   st.need_grad = 1;
-  MF_CK(cudaMemcpy(S.ctx.st, &st, sizeof(st), cudaMemcpyHostToDevice));
+  MF_CK(cudaMemcpyAsync(S.ctx.st, &st, sizeof(st), cudaMemcpyHostToDevice, S.stream));
   ProbParams p;
   memset(&p, 0, sizeof(p));
-  MF_CK(cudaMemcpy(S.ctx.prm, &p, sizeof(p), cudaMemcpyHostToDevice));
+  MF_CK(cudaMemcpyAsync(S.ctx.prm, &p, sizeof(p), cudaMemcpyHostToDevice, S.stream));
   if (x) {
-    MF_CK(cudaMemcpy(S.ctx.x, x, sizeof(double) * (size_t)Nx * Ny, cudaMemcpyHostToDevice));
+    MF_CK(cudaMemcpyAsync(S.ctx.x, x, sizeof(double) * (size_t)Nx * Ny, cudaMemcpyHostToDevice, S.stream));
     op->forward(S.stream, S.ctx.x, kGateAll, kQChiX, true);
     std::vector<cplx<T>> y2(std::max(M, 1));
     MF_CK(cudaMemcpyAsync(y2.data(), op->d_y2.p, sizeof(cplx<T>) * (size_t)M, cudaMemcpyDeviceToHost, S.stream));
@@ -556,7 +556,7 @@ int nufft_apply(const double* u, const double* v, const double* wstd, int M, int
   } else {
     std::vector<cplx<T>> y2(std::max(M, 1));
     for (int k = 0; k < M; ++k) y2[k] = mk<T>((T)r_r[k], (T)r_i[k]);
-    MF_CK(cudaMemcpy(op->d_y2.p, y2.data(), sizeof(cplx<T>) * (size_t)M, cudaMemcpyHostToDevice));
+    MF_CK(cudaMemcpyAsync(op->d_y2.p, y2.data(), sizeof(cplx<T>) * (size_t)M, cudaMemcpyHostToDevice, S.stream));
     op->adjoint(S.stream, nullptr, -1);
     MF_CK(cudaMemcpyAsync(x_out, S.ctx.dfdx, sizeof(double) * (size_t)Nx * Ny, cudaMemcpyDeviceToHost, S.stream));
     MF_CK(cudaStreamSynchronize(S.stream));
@@ -612,23 +612,52 @@ extern "C" int mfista_dft_apply(const double* A, int M, int N, const double* X, 
       q.active = 1;
       q.need_grad = 1;
     }
-    MF_CK(cudaMemcpy(S.ctx.st, st.data(), sizeof(ProbState) * B, cudaMemcpyHostToDevice));
-    MF_CK(cudaMemset(S.ctx.prm, 0, sizeof(ProbParams) * B));
-    MF_CK(cudaMemset(S.ctx.xa, 0, sizeof(double) * (size_t)B * N));  // anchor 0: the whole product is A x
+    MF_CK(cudaMemcpyAsync(S.ctx.st, st.data(), sizeof(ProbState) * B, cudaMemcpyHostToDevice, S.stream));
+    MF_CK(cudaMemsetAsync(S.ctx.prm, 0, sizeof(ProbParams) * B, S.stream));
+    MF_CK(cudaMemsetAsync(S.ctx.xa, 0, sizeof(double) * (size_t)B * N, S.stream));  // anchor 0: the whole product is A x
     if (!transpose) {
-      MF_CK(cudaMemcpy(S.ctx.x, X, sizeof(double) * (size_t)B * N, cudaMemcpyHostToDevice));
+      MF_CK(cudaMemcpyAsync(S.ctx.x, X, sizeof(double) * (size_t)B * N, cudaMemcpyHostToDevice, S.stream));
       op->forward(S.stream, S.ctx.x, kGateAll, kQChiX, true);  // stores y - A x with y = 0
       std::vector<double> r((size_t)B * M);
       MF_CK(cudaMemcpyAsync(r.data(), op->g.resid, sizeof(double) * r.size(), cudaMemcpyDeviceToHost, S.stream));
       MF_CK(cudaStreamSynchronize(S.stream));
       for (size_t i = 0; i < r.size(); ++i) out[i] = -r[i];
     } else {
-      MF_CK(cudaMemcpy(op->g.resid, X, sizeof(double) * (size_t)B * M, cudaMemcpyHostToDevice));
+      MF_CK(cudaMemcpyAsync(op->g.resid, X, sizeof(double) * (size_t)B * M, cudaMemcpyHostToDevice, S.stream));
       op->adjoint(S.stream, nullptr, -1);
       MF_CK(cudaMemcpyAsync(out, S.ctx.dfdx, sizeof(double) * (size_t)B * N, cudaMemcpyDeviceToHost, S.stream));
       MF_CK(cudaStreamSynchronize(S.stream));
     }
     if (op->device_error()) throw Error(MFISTA_ERR_CUDA, "a tensor-core GEMM wait timed out");
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
+extern "C" int mfista_dft_profile(const double* A, int M, int N, int B, int precision, int kernel, int reps,
+                                  double* ms_per_launch, double* bytes_per_launch) {
+  set_ok();
+  try {
+    if (M < 1 || N < 1 || B < 1 || !A) throw Error(MFISTA_ERR_ARG, "bad sizes or null pointer");
+    Solver S;
+    S.precision = MFISTA_FP64;
+    S.init_common(B, N, N, 1, kFormTSV, 100, nullptr);
+    std::vector<double> y(M, 0.0);
+    S.op.reset(new DftOp(S.ctx, A, y.data(), M, N, precision));
+    int slots = std::max({S.op->chi_slots(), S.op->tsv_slots(), S.img_blocks(), 1});
+    S.d_part.alloc(sizeof(double) * (size_t)kNumQ * B * slots);
+    S.ctx.part.p = S.d_part.as<double>();
+    S.ctx.part.slots = slots;
+    S.ctx.part.B = B;
+    MF_CK(cudaMemsetAsync(S.ctx.prm, 0, sizeof(ProbParams) * B, S.stream));
+    MF_CK(cudaMemsetAsync(S.ctx.z, 0, sizeof(double) * (size_t)B * N, S.stream));
+    double ms = 0, bytes = 0;
+    S.profile_kernel(kernel, 1, ms, bytes);  // warm
+    S.profile_kernel(kernel, std::max(1, reps), ms, bytes);
+    if (S.op->device_error()) throw Error(MFISTA_ERR_CUDA, "a tensor-core GEMM wait timed out");
+    if (ms_per_launch) *ms_per_launch = ms;
+    if (bytes_per_launch) *bytes_per_launch = bytes;
     return MFISTA_OK;
   } catch (const Error& e) {
     return fail(e.status, e.what(), false);
@@ -693,10 +722,10 @@ extern "C" int mfista_fgp_prox(const double* b, int NX, int NY, double lambda_l1
     memset(&st, 0, sizeof(st));
     st.active = 1;
     st.c = 1.0;
-    MF_CK(cudaMemcpy(S.ctx.prm, &p, sizeof(p), cudaMemcpyHostToDevice));
-    MF_CK(cudaMemcpy(S.ctx.st, &st, sizeof(st), cudaMemcpyHostToDevice));
-    MF_CK(cudaMemcpy(S.ctx.z, b, sizeof(double) * n, cudaMemcpyHostToDevice));
-    MF_CK(cudaMemset(S.ctx.dfdx, 0, sizeof(double) * n));
+    MF_CK(cudaMemcpyAsync(S.ctx.prm, &p, sizeof(p), cudaMemcpyHostToDevice, S.stream));
+    MF_CK(cudaMemcpyAsync(S.ctx.st, &st, sizeof(st), cudaMemcpyHostToDevice, S.stream));
+    MF_CK(cudaMemcpyAsync(S.ctx.z, b, sizeof(double) * n, cudaMemcpyHostToDevice, S.stream));
+    MF_CK(cudaMemsetAsync(S.ctx.dfdx, 0, sizeof(double) * n, S.stream));
     S.launch_fgp(S.stream);
     MF_CK(cudaMemcpyAsync(x_out, S.ctx.xnew, sizeof(double) * n, cudaMemcpyDeviceToHost, S.stream));
     MF_CK(cudaStreamSynchronize(S.stream));

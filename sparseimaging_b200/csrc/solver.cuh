@@ -179,6 +179,8 @@ struct Op {
   virtual int launches_refresh() const { return 0; }
   // non-zero when a device-side wait of the operator's kernels gave up
   virtual int device_error() { return 0; }
+  // outer iterations between anchor refreshes of the corrected forms
+  virtual int refresh_period() const { return 32; }
 };
 
 // ---------------------------------------------------------------------------
@@ -658,15 +660,18 @@ inline CUtensorMap bf16_tile_map(const void* base, int rows, int kpad, int box_r
 }
 
 // P[s][b][r] = sum_{k in split s} Amat[r][k] X[b][k] over K-major BF16 planes
+// (np = 2 or 3 planes per operand)
 struct TcGemm {
-  int rows = 0, kpad = 0, bpad = 0, nsplit = 1, kblocks = 0, kblocks_all = 0;
-  CUtensorMap ahi{}, alo{}, xhi{}, xlo{};
+  int np = 2, rows = 0, kpad = 0, bpad = 0, nsplit = 1, kblocks = 0, kblocks_all = 0;
+  tc::TcMaps maps{};
   DevMem part;  // [nsplit][bpad][rows] FP32
   int* err = nullptr;
 
+  int smem_bytes() const { return np == 3 ? tc::Ring<3>::kSmemBytes : tc::Ring<2>::kSmemBytes; }
+
   // split K so that the tiles cover the GPU's SMs about once (one CTA per SM)
-  void init(const void* a_hi, const void* a_lo, int rows_, int kpad_, const void* x_hi, const void* x_lo, int bpad_,
-            int* err_) {
+  void init(int np_, void* const* a_planes, int rows_, int kpad_, void* const* x_planes, int bpad_, int* err_) {
+    np = np_;
     rows = rows_;
     kpad = kpad_;
     bpad = bpad_;
@@ -679,25 +684,27 @@ struct TcGemm {
     nsplit = std::max(1, std::min(kblocks_all, sms / std::max(tiles, 1)));
     kblocks = cdiv(kblocks_all, nsplit);
     nsplit = cdiv(kblocks_all, kblocks);  // no empty split
-    ahi = bf16_tile_map(a_hi, rows, kpad, tc::kTM);
-    alo = bf16_tile_map(a_lo, rows, kpad, tc::kTM);
-    xhi = bf16_tile_map(x_hi, bpad, kpad, tc::kTN);
-    xlo = bf16_tile_map(x_lo, bpad, kpad, tc::kTN);
+    for (int p = 0; p < np; ++p) {
+      maps.a[p] = bf16_tile_map(a_planes[p], rows, kpad, tc::kTM);
+      maps.x[p] = bf16_tile_map(x_planes[p], bpad, kpad, tc::kTN);
+    }
     part.alloc(sizeof(float) * (size_t)nsplit * bpad * rows);
     MF_CK(cudaMemset(part.p, 0, part.bytes));
-    set_smem(tc::k_gemm_bf16x3, tc::kSmemBytes);
+    if (np == 3) set_smem(tc::k_gemm_split_bf16<3>, tc::Ring<3>::kSmemBytes);
+    else set_smem(tc::k_gemm_split_bf16<2>, tc::Ring<2>::kSmemBytes);
   }
 
   void launch(cudaStream_t s, const ProbState* st, int gate, int B) {
     tc::TcArgs a{part.as<float>(), rows, bpad, kblocks, kblocks_all, err};
-    tc::k_gemm_bf16x3<<<dim3(rows / tc::kTM, nsplit, bpad / tc::kTN), 128, tc::kSmemBytes, s>>>(ahi, alo, xhi, xlo,
-                                                                                               a, st, gate, B);
+    dim3 grid(rows / tc::kTM, nsplit, bpad / tc::kTN);
+    if (np == 3) tc::k_gemm_split_bf16<3><<<grid, 128, tc::Ring<3>::kSmemBytes, s>>>(maps, a, st, gate, B);
+    else tc::k_gemm_split_bf16<2><<<grid, 128, tc::Ring<2>::kSmemBytes, s>>>(maps, a, st, gate, B);
     MF_LAUNCH_CK();
   }
 
-  // algorithmic bytes of one launch: both A planes, both X planes, partials
+  // algorithmic bytes of one launch: the A planes, the X planes, the partials
   double bytes() const {
-    return 4.0 * rows * kpad + 4.0 * bpad * kpad + 4.0 * nsplit * bpad * rows;
+    return 2.0 * np * rows * kpad + 2.0 * np * bpad * kpad + 4.0 * nsplit * bpad * rows;
   }
 };
 
@@ -712,16 +719,19 @@ struct DftOp : Op {
   int B;
   bool gemm = false;     // batched problems: GEMMs instead of per-problem GEMVs
   int mchunk = 0, nmchunk = 0;
-  // split-BF16 form
+  // split-BF16 form (np planes per operand)
   bool tcm = false;
+  int np = 2;
   int mrow = 0, nk = 0, nrow = 0, mk = 0, bpad = 0;
-  DevMem rm_hi, rm_lo, cm_hi, cm_lo, xv_hi, xv_lo, xr_hi, xr_lo, d_axa, d_ra, d_ga, d_err;
+  DevMem rm[3], cm[3], xv[3], xr[3], d_axa, d_ra, d_ga, d_err;
   TcGemm fwd, adj;
 
   DftOp(Ctx& ctx, const double* A, const double* y, int M, int N, int precision = MFISTA_FP64) : c(ctx) {
     B = ctx.B;
-    tcm = precision == MFISTA_BF16X3;
-    if (!tcm && precision != MFISTA_FP64) throw Error(MFISTA_ERR_ARG, "the DFT operator runs in FP64 or BF16X3");
+    tcm = precision == MFISTA_BF16X3 || precision == MFISTA_BF16X6;
+    np = precision == MFISTA_BF16X6 ? 3 : 2;
+    if (!tcm && precision != MFISTA_FP64)
+      throw Error(MFISTA_ERR_ARG, "the DFT operator runs in FP64, BF16X3 or BF16X6");
     d_A.upload(A, (size_t)M * N);
     d_y.upload(y, M);
     g.A = d_A.as<double>();
@@ -743,6 +753,15 @@ struct DftOp : Op {
     g.az_part = d_part.as<double>();
     g.resid = d_resid.as<double>();
     if (tcm) setup_tc(M, N);
+    // the uploads above ran on the legacy stream; the solver's streams do
+    // not wait for it
+    MF_CK(cudaDeviceSynchronize());
+  }
+
+  static tc::Planes planes(DevMem* d, int np) {
+    tc::Planes q{};
+    for (int p = 0; p < np; ++p) q.p[p] = d[p].as<__nv_bfloat16>();
+    return q;
   }
 
   void setup_tc(int M, int N) {
@@ -752,32 +771,45 @@ struct DftOp : Op {
     mk = cdiv(M, tc::kTK) * tc::kTK;
     bpad = cdiv(B, tc::kTN) * tc::kTN;
     const size_t h = 2;  // bytes per BF16
-    rm_hi.alloc(h * mrow * nk);
-    rm_lo.alloc(h * mrow * nk);
-    cm_hi.alloc(h * nrow * mk);
-    cm_lo.alloc(h * nrow * mk);
-    k_split_matrix_launch(M, N);
-    xv_hi.alloc(h * bpad * nk);
-    xv_lo.alloc(h * bpad * nk);
-    xr_hi.alloc(h * bpad * mk);
-    xr_lo.alloc(h * bpad * mk);
-    for (DevMem* d : {&xv_hi, &xv_lo, &xr_hi, &xr_lo}) MF_CK(cudaMemset(d->p, 0, d->bytes));
+    for (int p = 0; p < np; ++p) {
+      rm[p].alloc(h * mrow * nk);
+      cm[p].alloc(h * nrow * mk);
+      xv[p].alloc(h * bpad * nk);
+      xr[p].alloc(h * bpad * mk);
+      MF_CK(cudaMemset(xv[p].p, 0, xv[p].bytes));
+      MF_CK(cudaMemset(xr[p].p, 0, xr[p].bytes));
+    }
+    dim3 grid(cdiv(std::max(mrow, mk), 32), cdiv(std::max(nrow, nk), 32));
+    if (np == 3)
+      tc::k_split_matrix<3><<<grid, 256>>>(g.A, M, N, mrow, nk, nrow, mk, planes(rm, 3), planes(cm, 3));
+    else
+      tc::k_split_matrix<2><<<grid, 256>>>(g.A, M, N, mrow, nk, nrow, mk, planes(rm, 2), planes(cm, 2));
+    MF_LAUNCH_CK();
     d_axa.alloc(sizeof(double) * (size_t)B * M);
     d_ra.alloc(sizeof(double) * (size_t)B * M);
     d_ga.alloc(sizeof(double) * (size_t)B * N);
     for (DevMem* d : {&d_axa, &d_ra, &d_ga}) MF_CK(cudaMemset(d->p, 0, d->bytes));
     d_err.alloc(sizeof(int));
     MF_CK(cudaMemset(d_err.p, 0, sizeof(int)));
-    fwd.init(rm_hi.p, rm_lo.p, mrow, nk, xv_hi.p, xv_lo.p, bpad, d_err.as<int>());
-    adj.init(cm_hi.p, cm_lo.p, nrow, mk, xr_hi.p, xr_lo.p, bpad, d_err.as<int>());
+    void *a_rm[3], *a_cm[3], *x_v[3], *x_r[3];
+    for (int p = 0; p < np; ++p) {
+      a_rm[p] = rm[p].p;
+      a_cm[p] = cm[p].p;
+      x_v[p] = xv[p].p;
+      x_r[p] = xr[p].p;
+    }
+    fwd.init(np, a_rm, mrow, nk, x_v, bpad, d_err.as<int>());
+    adj.init(np, a_cm, nrow, mk, x_r, bpad, d_err.as<int>());
     MF_CK(cudaDeviceSynchronize());
   }
 
-  void k_split_matrix_launch(int M, int N) {
-    dim3 grid(cdiv(std::max(mrow, mk), 32), cdiv(std::max(nrow, nk), 32));
-    tc::k_split_matrix<<<grid, 256>>>(g.A, M, N, mrow, nk, nrow, mk, rm_hi.as<__nv_bfloat16>(),
-                                      rm_lo.as<__nv_bfloat16>(), cm_hi.as<__nv_bfloat16>(),
-                                      cm_lo.as<__nv_bfloat16>());
+  void split_vectors(cudaStream_t s, const double* src, long sstride, const double* sub, int K, int kpad,
+                     DevMem* out, int gate) {
+    dim3 grid(cdiv(kpad, 256), bpad);
+    if (np == 3)
+      tc::k_split_vectors<3><<<grid, 256, 0, s>>>(src, sstride, sub, sstride, K, kpad, B, c.st, gate, planes(out, 3));
+    else
+      tc::k_split_vectors<2><<<grid, 256, 0, s>>>(src, sstride, sub, sstride, K, kpad, B, c.st, gate, planes(out, 2));
     MF_LAUNCH_CK();
   }
 
@@ -798,10 +830,7 @@ struct DftOp : Op {
       forward_fp64(s, src, gate, qchi, store);
       return;
     }
-    tc::k_split_vectors<<<dim3(cdiv(nk, 256), bpad), 256, 0, s>>>(src, c.xstride, c.xa, c.xstride, g.N, nk, B, c.st,
-                                                                   gate, xv_hi.as<__nv_bfloat16>(),
-                                                                   xv_lo.as<__nv_bfloat16>());
-    MF_LAUNCH_CK();
+    split_vectors(s, src, c.xstride, c.xa, g.N, nk, xv, gate);
     fwd.launch(s, c.st, gate, B);
     k_dft_tc_resid<<<dim3(std::max(1, cdiv(g.M, 256)), B), 256, 0, s>>>(fwd.part.as<float>(), fwd.nsplit, bpad, mrow,
                                                                         d_axa.as<double>(), g, c.st, gate, c.part,
@@ -811,10 +840,7 @@ struct DftOp : Op {
 
   void adjoint(cudaStream_t s, const double* z_tsv, int qtsv) override {
     if (tcm) {
-      tc::k_split_vectors<<<dim3(cdiv(mk, 256), bpad), 256, 0, s>>>(g.resid, g.M, d_ra.as<double>(), g.M, g.M, mk, B,
-                                                                     c.st, kGateGrad, xr_hi.as<__nv_bfloat16>(),
-                                                                     xr_lo.as<__nv_bfloat16>());
-      MF_LAUNCH_CK();
+      split_vectors(s, g.resid, g.M, d_ra.as<double>(), g.M, mk, xr, kGateGrad);
       adj.launch(s, c.st, kGateGrad, B);
       k_dft_tc_atr_finish<<<dim3(cdiv(g.N, 256), B), 256, 0, s>>>(adj.part.as<float>(), adj.nsplit, bpad, nrow,
                                                                    d_ga.as<double>(), g.N, c.dfdx, c.xstride, z_tsv,
@@ -850,6 +876,9 @@ struct DftOp : Op {
 
   bool corrected() const override { return tcm; }
   int launches_refresh() const override { return tcm ? 4 : 0; }
+  // the two-plane products (~2^-16) need a closer anchor than the
+  // three-plane ones to reach 1e-6 of the FP64 objective
+  int refresh_period() const override { return np == 2 ? 8 : 32; }
 
   // FP64 anchor terms: ax_a = A x_a, r_a = y - ax_a, g_a = A^T r_a
   void refresh_anchor(cudaStream_t s, int gate) override {
@@ -1000,13 +1029,18 @@ struct Solver {
     ctx.part.slots = slots;
     ctx.part.B = ctx.B;
     if (form == kFormTV) setup_fgp();
-    refresh_every = op->corrected() ? 32 : 0;
+    refresh_every = op->corrected() ? op->refresh_period() : 0;
+    if (const char* re = getenv("MFISTA_REFRESH_EVERY"))  // anchor refresh period (tuning)
+      if (op->corrected() && atoi(re) > 0) refresh_every = atoi(re);
     per_step_launches = op->launches_forward() * 2 + op->launches_adjoint() + 3 + (form == kFormTV ? 1 : 0) +
                         (op->corrected() ? 1 + op->launches_refresh() : 0);
     fixed_launches = 2 * (op->launches_forward() + 2) + 1;
     const char* hl = getenv("MFISTA_HOST_LOOP");
     host_loop = hl && hl[0] == '1';
     build_graph();
+    // set-up copies and memsets ran on the legacy stream, which the solver's
+    // non-blocking streams do not wait for
+    MF_CK(cudaDeviceSynchronize());
   }
 
   template <typename K> int max_clusters(K kern, int cs, size_t smem) {

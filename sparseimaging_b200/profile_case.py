@@ -9,7 +9,9 @@ plan's, and set MFISTA_HOST_LOOP=1: ncu profiles the kernels of an ordinary
 graph but not those inside a conditional WHILE body.
 
 --case lambda-grid: the 128x128, M = 8100, 64-problem lambda grid that
-bench.py times; --case config0: the 64x64 single problem.  Without
+bench.py times; --case config0: the 64x64 single problem; --case dft: the
+batched DFT GEMMs (A 8000 x 4096, --problems right-hand sides) timed alone,
+--precision 64 for FP64 or 32 for the tensor-core split-BF16 form.  Without
 --kernel it runs one batched solve of --iters MFISTA iterations; with
 --kernel k it times that operator kernel alone (see mfista_plan_profile).
 """
@@ -25,7 +27,7 @@ import numpy as np
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--case", default="lambda-grid", choices=["lambda-grid", "config0"])
+    ap.add_argument("--case", default="lambda-grid", choices=["lambda-grid", "config0", "dft"])
     ap.add_argument("--precision", type=int, default=64, choices=[32, 64])
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--kernel", type=int, default=-1)
@@ -41,6 +43,18 @@ def main():
     os.environ.setdefault("MFISTA_QUIET", "1")
     import sparseimaging_b200 as si
     from sparseimaging_b200 import synth
+    if a.case == "dft":
+        # 64x64 image, 4000 visibilities from 10 stations: A is 8000 x 4096
+        p = synth.dft_problem()
+        prec = {64: si.FP64, 32: si.BF16X3}[a.precision]
+        out = {"case": "dft", "precision": "fp64" if prec == si.FP64 else "bf16x3", "M": p.A.shape[0],
+               "N": p.A.shape[1], "problems": a.problems}
+        for k in (0, 1) if a.kernel < 0 else (a.kernel,):
+            ms, by = si.dft_profile(p.A, a.problems, k, precision=prec, reps=a.reps)
+            out[f"kernel{k}"] = {"ms_per_launch": ms, "bytes_per_launch": by, "gbs": by / ms / 1e6,
+                                 "tflops": 2.0 * p.A.shape[0] * p.A.shape[1] * a.problems / ms / 1e9}
+        print(json.dumps(out))
+        return
     p = synth.lambda_grid_problem() if a.case == "lambda-grid" else synth.config0()
     nx = p.nx
     w2 = 1 / p.vis_std ** 2
