@@ -584,35 +584,28 @@ __global__ void __launch_bounds__(256, SharedChunk<T>::kInterpMinBlocks) k_nufft
 // broadcasts, so a point that misses a cell costs one mask test.
 constexpr int kSpreadTile = 16;
 
-template <typename T>
-__global__ void __launch_bounds__(256, 2) k_nufft_spread_shared(NufftGeom<T> geo, const cplx<T>* __restrict__ y2,
-                                                                cplx<T>* __restrict__ gall, long gstride, int nx,
-                                                                int ny, int ntiles, const ProbState* __restrict__ st,
-                                                                int gate, int B) {
-  constexpr int PB = SharedChunk<T>::kSpread;
-  constexpr int P = 32;
+// shared-memory staging of one CTA of the spreading kernel
+template <typename T, int PB> struct SpreadSmem {
+  static constexpr int P = 32;  // points staged per round
+  int ox[P], oy[P];             // 11 - mx, 11 - my
+  unsigned int mask[P];         // rows (low 16 bits) | cols (high 16 bits)
+  T wx[P][kTaps], wy[P][kTaps];
+  __align__(16) cplx<T> r[P][PB];
+  int list[PB];                 // the chunk's active problems, compacted
+  int cnt;
+};
+
+// Accumulates the tile's segment of points for the first NB active problems
+// of the chunk (NB >= cnt) and writes the cluster's sum.  NB is a compile-time
+// bound so that a chunk with few active problems (the tail of a lambda grid)
+// runs a short FMA loop while a full chunk keeps a fully unrolled one.
+template <typename T, int PB, int NB>
+__device__ __forceinline__ void spread_tile(const NufftGeom<T>& geo, const cplx<T>* __restrict__ y2,
+                                            cplx<T>* __restrict__ gall, long gstride, int nx, int ny, int tile,
+                                            int b0, int cnt, SpreadSmem<T, PB>& sm, cplx<T>* s_acc,
+                                            cg::cluster_group& cluster, int rank, int csize) {
+  constexpr int P = SpreadSmem<T, PB>::P;
   constexpr int TILE = kSpreadTile;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cplx<T>* s_acc = reinterpret_cast<cplx<T>*>(smem_raw);  // [PB][256] segment accumulators
-  __shared__ int s_ox[P], s_oy[P];          // 11 - mx, 11 - my
-  __shared__ unsigned int s_mask[P];        // rows (low 16 bits) | cols (high 16 bits)
-  __shared__ T s_wx[P][kTaps], s_wy[P][kTaps];
-  __shared__ __align__(16) cplx<T> s_r[P][PB];
-  __shared__ int s_act[PB];
-  cg::cluster_group cluster = cg::this_cluster();
-  const int rank = (int)cluster.block_rank();
-  const int csize = (int)cluster.num_blocks();
-  const int b0 = blockIdx.y * PB;
-  if (threadIdx.x < PB) {
-    int b = b0 + threadIdx.x;
-    s_act[threadIdx.x] = (b < B && gate_ok(st[b], gate)) ? 1 : 0;
-  }
-  __syncthreads();
-  int any = 0;
-#pragma unroll
-  for (int i = 0; i < PB; ++i) any |= s_act[i];
-  if (!any) return;  // uniform over the cluster: same problem chunk
-  const int tile = blockIdx.x / csize;
   const int ntc = (ny + 1 + TILE - 1) / TILE;
   const int tr = tile / ntc, tc = tile - tr * ntc;
   const int ty = threadIdx.x / TILE, tx = threadIdx.x - ty * TILE;
@@ -621,58 +614,64 @@ __global__ void __launch_bounds__(256, 2) k_nufft_spread_shared(NufftGeom<T> geo
   const bool valid = row < 2 * nx && col <= ny;
   const int mrow = row < nx ? row : row - 2 * nx;
   const int mcol = col < ny ? col : -ny;
-  T ar[PB], ai[PB];
+  T ar[NB], ai[NB];
 #pragma unroll
-  for (int i = 0; i < PB; ++i) ar[i] = ai[i] = 0;
+  for (int i = 0; i < NB; ++i) ar[i] = ai[i] = 0;
   const int lbeg = geo.tile_ptr[tile], lend = geo.tile_ptr[tile + 1];
   const int seg = (lend - lbeg + csize - 1) / csize;
   const int beg = min(lend, lbeg + rank * seg), end = min(lend, beg + seg);
   for (int c0 = beg; c0 < end; c0 += P) {
     const int np = min(P, end - c0);
     __syncthreads();
-    if (threadIdx.x < np) {
-      const int t = threadIdx.x;
-      const int k = geo.tile_pts[c0 + t];
-      const int mx = geo.mx[k], my = geo.my[k];
-      s_ox[t] = (kMSP - 1) - mx;
-      s_oy[t] = (kMSP - 1) - my;
-      // tile rows / columns reached by the direct or mirrored footprint
-      unsigned int rm = 0, cm = 0;
-      for (int q = 0; q < TILE; ++q) {
-        int r = row0 + q, cc = col0 + q;
-        int mr = r < nx ? r : r - 2 * nx;
-        int mc = cc < ny ? cc : -ny;
-        if (r < 2 * nx && ((unsigned)(mr - mx + (kMSP - 1)) < (unsigned)kTaps ||
-                           (unsigned)(-mr - mx + (kMSP - 1)) < (unsigned)kTaps))
-          rm |= 1u << q;
-        if (cc <= ny && ((unsigned)(mc - my + (kMSP - 1)) < (unsigned)kTaps ||
-                         (unsigned)(-mc - my + (kMSP - 1)) < (unsigned)kTaps))
-          cm |= 1u << q;
+    {
+      // tile rows / columns reached by each point's direct or mirrored
+      // footprint: warp w takes points w, w + 8, ...; lane q < 16 tests tile
+      // row q, lane 16 + q tile column q, and one ballot gives the mask
+      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      const int q = lane & (TILE - 1);
+      const int r = row0 + q, cc = col0 + q;
+      const int mr = r < nx ? r : r - 2 * nx;
+      const int mc = cc < ny ? cc : -ny;
+      for (int t = warp; t < np; t += 8) {
+        const int k = geo.tile_pts[c0 + t];
+        const int mx = geo.mx[k], my = geo.my[k];
+        bool hit;
+        if (lane < TILE)
+          hit = r < 2 * nx && ((unsigned)(mr - mx + (kMSP - 1)) < (unsigned)kTaps ||
+                               (unsigned)(-mr - mx + (kMSP - 1)) < (unsigned)kTaps);
+        else
+          hit = cc <= ny && ((unsigned)(mc - my + (kMSP - 1)) < (unsigned)kTaps ||
+                             (unsigned)(-mc - my + (kMSP - 1)) < (unsigned)kTaps);
+        const unsigned int m = __ballot_sync(0xffffffffu, hit);
+        if (lane == 0) {
+          sm.ox[t] = (kMSP - 1) - mx;
+          sm.oy[t] = (kMSP - 1) - my;
+          sm.mask[t] = m;
+        }
       }
-      s_mask[t] = rm | (cm << 16);
     }
     for (int t = threadIdx.x; t < np * kTaps; t += blockDim.x) {
       int pp = t / kTaps, j = t - pp * kTaps;
       int k = geo.tile_pts[c0 + pp];
-      s_wx[pp][j] = geo.wx[(size_t)k * kTaps + j];
-      s_wy[pp][j] = geo.wy[(size_t)k * kTaps + j];
+      sm.wx[pp][j] = geo.wx[(size_t)k * kTaps + j];
+      sm.wy[pp][j] = geo.wy[(size_t)k * kTaps + j];
     }
-    for (int t = threadIdx.x; t < np * PB; t += blockDim.x) {
-      int pp = t / PB, i = t - pp * PB;
+    for (int t = threadIdx.x; t < np * NB; t += blockDim.x) {
+      int pp = t / NB, i = t - pp * NB;
       int k = geo.tile_pts[c0 + pp];
       cplx<T> r = mk<T>(0, 0);
-      if (s_act[i]) {
-        r = y2[(size_t)(b0 + i) * geo.y2_bstride + k];
+      if (i < cnt) {
+        r = y2[(size_t)(b0 + sm.list[i]) * geo.y2_bstride + k];
         r.y = -r.y;  // NU_SIGN * Fin_i
       }
-      s_r[pp][i] = r;
+      sm.r[pp][i] = r;
     }
     __syncthreads();
     if (valid) {
       const unsigned int mybits = (1u << ty) | (1u << (16 + tx));
       for (int pp = 0; pp < np; ++pp) {
-        if ((s_mask[pp] & mybits) != mybits) continue;
-        const int ox = s_ox[pp], oy = s_oy[pp];
+        if ((sm.mask[pp] & mybits) != mybits) continue;
+        const int ox = sm.ox[pp], oy = sm.oy[pp];
         const int lxd = mrow + ox, lyd = mcol + oy;
         const int lxm = ox - mrow, lym = oy - mcol;
         const bool d = (unsigned)lxd < (unsigned)kTaps && (unsigned)lyd < (unsigned)kTaps;
@@ -684,12 +683,12 @@ __global__ void __launch_bounds__(256, 2) k_nufft_spread_shared(NufftGeom<T> geo
           const bool use_m = (pass == 0) ? mfirst : (mi && !mfirst);
           const bool use_d = (pass == 0) ? (d && !mfirst) : (d && mfirst);
           if (!(use_m || use_d)) continue;
-          const T w = use_m ? s_wy[pp][lym] * s_wx[pp][lxm] : s_wy[pp][lyd] * s_wx[pp][lxd];
+          const T w = use_m ? sm.wy[pp][lym] * sm.wx[pp][lxm] : sm.wy[pp][lyd] * sm.wx[pp][lxd];
           const T hw = w * T(0.5);
           const T hwi = use_m ? -hw : hw;
 #pragma unroll
-          for (int i = 0; i < PB; ++i) {
-            cplx<T> r = s_r[pp][i];
+          for (int i = 0; i < NB; ++i) {
+            cplx<T> r = sm.r[pp][i];
             ar[i] += r.x * hw;
             ai[i] += r.y * hwi;
           }
@@ -699,13 +698,13 @@ __global__ void __launch_bounds__(256, 2) k_nufft_spread_shared(NufftGeom<T> geo
   }
   // segment accumulators -> shared memory; rank 0 adds ranks 1.. in order
 #pragma unroll
-  for (int i = 0; i < PB; ++i) s_acc[i * 256 + threadIdx.x] = mk<T>(ar[i], ai[i]);
+  for (int i = 0; i < NB; ++i) s_acc[i * 256 + threadIdx.x] = mk<T>(ar[i], ai[i]);
   cluster.sync();
   if (rank == 0) {
     for (int r = 1; r < csize; ++r) {
       const cplx<T>* peer = cluster.map_shared_rank(s_acc, r);
 #pragma unroll
-      for (int i = 0; i < PB; ++i) {
+      for (int i = 0; i < NB; ++i) {
         cplx<T> v = peer[i * 256 + threadIdx.x];
         ar[i] += v.x;
         ai[i] += v.y;
@@ -713,11 +712,49 @@ __global__ void __launch_bounds__(256, 2) k_nufft_spread_shared(NufftGeom<T> geo
     }
     if (valid) {
 #pragma unroll
-      for (int i = 0; i < PB; ++i)
-        if (s_act[i]) gall[(size_t)(b0 + i) * gstride + (size_t)row * (ny + 1) + col] = mk<T>(ar[i], ai[i]);
+      for (int i = 0; i < NB; ++i)
+        if (i < cnt) gall[(size_t)(b0 + sm.list[i]) * gstride + (size_t)row * (ny + 1) + col] = mk<T>(ar[i], ai[i]);
     }
   }
   cluster.sync();  // peers' shared memory must stay alive until rank 0 is done
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_nufft_spread_shared(NufftGeom<T> geo, const cplx<T>* __restrict__ y2,
+                                                                cplx<T>* __restrict__ gall, long gstride, int nx,
+                                                                int ny, int ntiles, const ProbState* __restrict__ st,
+                                                                int gate, int B) {
+  constexpr int PB = SharedChunk<T>::kSpread;
+  static_assert(kSpreadTile == 16, "the footprint masks use 16 row and 16 column bits");
+  static_assert(PB % 4 == 0, "problem chunks are multiples of 4");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* s_acc = reinterpret_cast<cplx<T>*>(smem_raw);  // [PB][256] segment accumulators
+  __shared__ SpreadSmem<T, PB> sm;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  const int csize = (int)cluster.num_blocks();
+  const int b0 = blockIdx.y * PB;
+  if (threadIdx.x == 0) {
+    int n = 0;
+    for (int i = 0; i < PB; ++i) {
+      int b = b0 + i;
+      if (b < B && gate_ok(st[b], gate)) sm.list[n++] = i;
+    }
+    sm.cnt = n;
+  }
+  __syncthreads();
+  const int cnt = sm.cnt;
+  if (cnt == 0) return;  // uniform over the cluster: same problem chunk
+  const int tile = blockIdx.x / csize;
+  // accumulator slot i holds problem b0 + list[i]: the smallest unrolled
+  // width that holds the chunk's active problems
+  if (cnt <= 4)
+    spread_tile<T, PB, 4>(geo, y2, gall, gstride, nx, ny, tile, b0, cnt, sm, s_acc, cluster, rank, csize);
+  else if (PB > 8 && cnt <= 8)
+    spread_tile<T, PB, (PB > 8 ? 8 : PB)>(geo, y2, gall, gstride, nx, ny, tile, b0, cnt, sm, s_acc, cluster, rank,
+                                          csize);
+  else
+    spread_tile<T, PB, PB>(geo, y2, gall, gstride, nx, ny, tile, b0, cnt, sm, s_acc, cluster, rank, csize);
 }
 
 }  // namespace mf

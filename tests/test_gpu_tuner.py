@@ -68,9 +68,12 @@ def test_tuned_plan_solves_like_default(gpulib, c0, precision):
     assert shapes["rows_per_cta"] >= 1 and shapes["cols_per_cta"] >= 1
     assert all(v > 0 for v in ms.values())
     X, R = _solve(plan, probs)
-    tol = 1e-10 if precision == "fp64" else 1e-4
+    # FP64: rounding-level moves; FP32: regrouped FP32 sums move 150-iteration
+    # images by ~1e-4 and objectives by ~1e-7
+    xtol, ftol = (1e-10, 1e-12) if precision == "fp64" else (2e-3, 1e-6)
     for b in range(len(probs)):
-        assert rel(X[b], X0[b]) < tol
+        assert rel(X[b], X0[b]) < xtol
+        assert abs(R[b]["finalcost"] - R0[b]["finalcost"]) <= ftol * R0[b]["finalcost"]
     plan.close()
 
 
