@@ -273,6 +273,29 @@ int mfista_fgp_prox(const double *b, int NX, int NY, double lambda_l1, double la
 int mfista_nufft_lipschitz(const double *u_dx, const double *v_dy, const double *vis_std,
                            int M, int Nx, int Ny, int iters, double *lip_out);
 
+/* Learned warm start (no counterpart in the reference): a U-Net with 4
+ * levels of 16-32-64-128 channels, BF16 weights and FP32 accumulation, that
+ * maps a problem's dirty image and dirty beam (2 input channels, H x W, H
+ * and W multiples of 8) to an initial image clamped to >= 0.  Forward,
+ * backward and Adam run on the GPU (deterministic).  Arrays are host float
+ * arrays: inputs [n][2][H][W], images [n][H][W], parameters in the layout
+ * of csrc/unet.cu (per 3x3 layer: weights [cout][cin][3][3], bias [cout];
+ * then the 1x1 head's 16 weights and bias).  Status: 0 or an mfista_status
+ * (details from mfista_unet_last_error). */
+void *mfista_unet_create(int H, int W, int batch_max);
+void mfista_unet_destroy(void *net);
+long mfista_unet_param_count(void *net);
+int mfista_unet_get_params(void *net, float *out);
+int mfista_unet_set_params(void *net, const float *in);
+int mfista_unet_forward(void *net, const float *in, int n, float *out);
+/* loss = mean squared error of the unclamped output against target;
+ * grad [param_count] (may be NULL) */
+int mfista_unet_grad(void *net, const float *in, const float *target, int n, float *loss, float *grad);
+/* one Adam step (beta 0.9 / 0.999) with learning rate lr; reports the loss */
+int mfista_unet_train_step(void *net, const float *in, const float *target, int n, float lr, float *loss);
+int mfista_unet_last_status(void);
+const char *mfista_unet_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

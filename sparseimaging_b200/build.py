@@ -14,7 +14,7 @@ import sys
 PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libmfista_b200.so")
-SOURCES = ["mfista_b200.cu", "nufft_noalloc.cu"]
+SOURCES = ["mfista_b200.cu", "nufft_noalloc.cu", "unet.cu"]
 HEADERS = ["common.cuh", "fft_smem.cuh", "nufft_ops.cuh", "fftvar_ops.cuh", "dft_ops.cuh",
            "mfista_ops.cuh", "fgp.cuh", "solver.cuh"]
 

@@ -1,0 +1,253 @@
+"""Learned warm start for the NUFFT solves (no counterpart in the reference).
+
+A U-Net (csrc/unet.cu: 4 levels, 16-32-64-128 channels, BF16 weights, FP32
+accumulation, trained on the GPU by the library's own kernels) maps the
+dirty image A^H W^2 y and the dirty beam A^H W^2 1 of a problem to an
+initial image.  MFISTA then runs from that image with the reference's own
+stopping rule, so the solver stays the judge; per problem the start is used
+only when its objective is below that of the zero image (zero init is the
+fallback, `choose_starts`).
+
+Input scaling: both maps are divided by the beam's peak (a unit point
+source then has peak 1 in the dirty image), and the dirty image and the
+target solution by the dirty image's peak, so the network sees O(1) values;
+its output is scaled back.
+
+    python -m sparseimaging_b200.warmstart --train   (on a GPU: makes the
+        training set with the FP64 solver and writes WEIGHTS)
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import time
+
+import numpy as np
+
+from . import MfistaError, nufft_adjoint, synth
+from . import lib as _lib_loader
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+WEIGHTS = os.path.join(HERE, "data", "unet_warmstart_128.npy")
+TRAIN_LAMBDA = 1e-3  # training targets: lambda_l1 = lambda_tsv = 1e-3 max|A^H W^2 y|
+
+_bound = False
+
+
+def _lib():
+    global _bound
+    L = _lib_loader()
+    if not _bound:
+        vp, fp = C.c_void_p, C.POINTER(C.c_float)
+        L.mfista_unet_create.restype = vp
+        L.mfista_unet_create.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.mfista_unet_destroy.restype = None
+        L.mfista_unet_destroy.argtypes = [vp]
+        L.mfista_unet_param_count.restype = C.c_long
+        L.mfista_unet_param_count.argtypes = [vp]
+        L.mfista_unet_get_params.restype = C.c_int
+        L.mfista_unet_get_params.argtypes = [vp, fp]
+        L.mfista_unet_set_params.restype = C.c_int
+        L.mfista_unet_set_params.argtypes = [vp, fp]
+        L.mfista_unet_forward.restype = C.c_int
+        L.mfista_unet_forward.argtypes = [vp, fp, C.c_int, fp]
+        L.mfista_unet_grad.restype = C.c_int
+        L.mfista_unet_grad.argtypes = [vp, fp, fp, C.c_int, fp, fp]
+        L.mfista_unet_train_step.restype = C.c_int
+        L.mfista_unet_train_step.argtypes = [vp, fp, fp, C.c_int, C.c_float, fp]
+        L.mfista_unet_last_status.restype = C.c_int
+        L.mfista_unet_last_error.restype = C.c_char_p
+        _bound = True
+    return L
+
+
+def _f(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _ok(st):
+    if st != 0:
+        raise MfistaError(st, _lib().mfista_unet_last_error().decode())
+
+
+class UNet:
+    """The GPU U-Net: forward, gradients and Adam steps."""
+
+    def __init__(self, H, W, batch_max=8):
+        L = _lib()
+        self.H, self.W, self.batch_max = H, W, batch_max
+        self.h = L.mfista_unet_create(H, W, batch_max)
+        if not self.h:
+            _ok(L.mfista_unet_last_status() or 1)
+        self.n = int(L.mfista_unet_param_count(self.h))
+
+    def params(self):
+        out = np.zeros(self.n, np.float32)
+        _ok(_lib().mfista_unet_get_params(self.h, _fp(out)))
+        return out
+
+    def set_params(self, p):
+        p = _f(p)
+        if p.size != self.n:
+            raise ValueError(f"expected {self.n} parameters, got {p.size}")
+        _ok(_lib().mfista_unet_set_params(self.h, _fp(p)))
+
+    def forward(self, x):
+        """Initial images [n][H][W] (clamped >= 0) for inputs [n][2][H][W]."""
+        x = _f(x).reshape(-1, 2, self.H, self.W)
+        out = np.zeros((x.shape[0], self.H, self.W), np.float32)
+        for i in range(0, x.shape[0], self.batch_max):
+            xb = np.ascontiguousarray(x[i:i + self.batch_max])
+            ob = np.zeros((xb.shape[0], self.H, self.W), np.float32)
+            _ok(_lib().mfista_unet_forward(self.h, _fp(xb), xb.shape[0], _fp(ob)))
+            out[i:i + xb.shape[0]] = ob
+        return out
+
+    def grad(self, x, t):
+        x, t = _f(x), _f(t)
+        loss = C.c_float(0)
+        g = np.zeros(self.n, np.float32)
+        _ok(_lib().mfista_unet_grad(self.h, _fp(x), _fp(t), x.shape[0], C.byref(loss), _fp(g)))
+        return float(loss.value), g
+
+    def train_step(self, x, t, lr):
+        x, t = _f(x), _f(t)
+        loss = C.c_float(0)
+        _ok(_lib().mfista_unet_train_step(self.h, _fp(x), _fp(t), x.shape[0], lr, C.byref(loss)))
+        return float(loss.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib().mfista_unet_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def dirty_inputs(u_dx, v_dy, vis_r, vis_i, vis_std, nx):
+    """(network input [2][nx][nx], scale): dirty image and dirty beam over
+    the beam's peak, the image also over its own peak (= scale)."""
+    w2 = 1.0 / np.asarray(vis_std, np.float64) ** 2
+    dirty = nufft_adjoint(u_dx, v_dy, nx, nx, np.asarray(vis_r) * w2, np.asarray(vis_i) * w2)
+    beam = nufft_adjoint(u_dx, v_dy, nx, nx, w2, np.zeros_like(w2))
+    peak = beam.max()
+    dirty, beam = dirty / peak, beam / peak
+    scale = max(float(np.abs(dirty).max()), 1e-30)
+    x = np.stack([dirty.reshape(nx, nx) / scale, beam.reshape(nx, nx)])
+    return x.astype(np.float32), scale
+
+
+def predict(net, u_dx, v_dy, vis_r, vis_i, vis_std, nx):
+    """Initial image [nx*nx] (>= 0) for one problem."""
+    x, scale = dirty_inputs(u_dx, v_dy, vis_r, vis_i, vis_std, nx)
+    return net.forward(x[None])[0].reshape(-1).astype(np.float64) * scale
+
+
+def choose_starts(geo, problems, x_warm, precision=None):
+    """Per problem, x_warm where its objective is below the zero image's,
+    else zero (each objective from one evaluation at the start, no
+    iteration).  geo = (u, v, vis_r, vis_i, vis_std, nx, ny).  Returns
+    ([B * N] starts, [B] bool used)."""
+    from . import FP64, nufft_batch
+    B = len(problems)
+    at0 = [dict(p, maxiter=0, target_cost=0.0) for p in problems]
+    prec = FP64 if precision is None else precision
+    _, Rw = nufft_batch(*geo, at0, 0.0, xinit=np.tile(x_warm, B), precision=prec)
+    _, Rz = nufft_batch(*geo, at0, 0.0, precision=prec)
+    used = np.array([rw["finalcost"] < rz["finalcost"] for rw, rz in zip(Rw, Rz)])
+    starts = np.where(used[:, None], np.asarray(x_warm)[None, :], 0.0).reshape(-1)
+    return starts, used
+
+
+def load(nx=128, batch_max=8, path=WEIGHTS):
+    """The trained network (raises if the weights file is absent)."""
+    net = UNet(nx, nx, batch_max)
+    net.set_params(np.load(path))
+    return net
+
+
+# ---------------------------------------------------------------------------
+# training set: seeded synthetic skies solved by the FP64 solver
+# ---------------------------------------------------------------------------
+def training_problem(seed, nx=128):
+    """A seeded sky and uv coverage shaped like the benchmark's (8-12
+    stations, 180 hour angles), different per seed."""
+    rng = np.random.default_rng(seed)
+    return synth.lambda_grid_problem(seed=seed, nx=nx, n_stations=int(rng.integers(8, 13)), n_hours=180)
+
+
+def make_training_set(seeds, nx=128, iters=1500, batch=32, lam_rel=TRAIN_LAMBDA):
+    """(inputs [n][2][nx][nx], targets [n][nx][nx]) for the given seeds: the
+    targets are FP64 MFISTA solutions (`iters` iterations) at
+    lambda_l1 = lambda_tsv = lam_rel * max|A^H W^2 y|."""
+    from . import FP64, nufft_batch, nufft_lipschitz
+    X, T = [], []
+    for i in range(0, len(seeds), batch):
+        ps = [training_problem(s, nx) for s in seeds[i:i + batch]]
+        cat = lambda f: np.concatenate([getattr(p, f) for p in ps])
+        off = np.concatenate([[0], np.cumsum([p.m for p in ps])]).astype(np.int32)
+        problems, scales = [], []
+        for p in ps:
+            x, scale = dirty_inputs(p.u_dx, p.v_dy, p.vis_r, p.vis_i, p.vis_std, nx)
+            w2 = 1 / p.vis_std ** 2
+            g0 = nufft_adjoint(p.u_dx, p.v_dy, nx, nx, p.vis_r * w2, p.vis_i * w2)
+            lam = lam_rel * float(np.abs(g0).max())
+            lip = nufft_lipschitz(p.u_dx, p.v_dy, p.vis_std, nx, nx, iters=20)
+            problems.append(dict(lambda_l1=lam, lambda_tsv=lam, cinit=lip, maxiter=iters, nonneg_flag=1))
+            X.append(x)
+            scales.append(scale)
+        Xs, _ = nufft_batch(cat("u_dx"), cat("v_dy"), cat("vis_r"), cat("vis_i"), cat("vis_std"), nx, nx,
+                            problems, 1e-7, pt_off=off, precision=FP64)
+        for k, s in enumerate(scales):
+            T.append((Xs[k].reshape(nx, nx) / s).astype(np.float32))
+    return np.stack(X), np.stack(T)
+
+
+def train(X, T, steps=400, batch=8, lr=1e-3, seed=0, net=None, log=None):
+    """Adam on random minibatches (learning rate / 10 for the last 20 %);
+    returns the network and the loss history."""
+    net = net or UNet(X.shape[-2], X.shape[-1], batch)
+    rng = np.random.default_rng(seed)
+    hist = []
+    for s in range(steps):
+        idx = rng.choice(X.shape[0], size=min(batch, X.shape[0]), replace=False)
+        hist.append(net.train_step(X[idx], T[idx], lr * (0.1 if s >= int(0.8 * steps) else 1.0)))
+        if log and (s % 100 == 0 or s == steps - 1):
+            log(f"step {s} loss {hist[-1]:.4g}")
+    return net, hist
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", action="store_true")
+    ap.add_argument("--n-train", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=1500)
+    ap.add_argument("--out", default=WEIGHTS)
+    ap.add_argument("--iters", type=int, default=1500, help="FP64 MFISTA iterations per training target")
+    ap.add_argument("--lam", type=float, default=TRAIN_LAMBDA, help="training lambdas relative to max|A^H W^2 y|")
+    a = ap.parse_args()
+    os.environ.setdefault("MFISTA_QUIET", "1")
+    if not a.train:
+        ap.print_help()
+        return
+    t0 = time.time()
+    X, T = make_training_set(list(range(1000, 1000 + a.n_train)), iters=a.iters, lam_rel=a.lam)
+    t1 = time.time()
+    net, hist = train(X, T, steps=a.steps, log=print)
+    t2 = time.time()
+    os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
+    np.save(a.out, net.params())
+    print(json.dumps({"n_train": a.n_train, "steps": a.steps, "iters": a.iters, "lam": a.lam,
+                      "data_s": t1 - t0, "train_s": t2 - t1,
+                      "loss_first": hist[0], "loss_last": float(np.mean(hist[-50:]))}))
+
+
+if __name__ == "__main__":
+    main()
