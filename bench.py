@@ -68,6 +68,23 @@ def workload(seed):
     return synth.lambda_grid_problem(seed=seed, nx=NX, n_stations=N_STATIONS, n_hours=N_HOURS)
 
 
+def max_over_ranks(values, world, dist=None, device=None):
+    """Element-wise maximum of a list of floats over all ranks (one
+    all-reduce; every rank must call it at the same point)."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def weak_rate(units_per_rank, world, seconds):
+    """Whole-job rate when every rank processed `units_per_rank` in at most
+    `seconds` (the slowest rank's time)."""
+    return world * units_per_rank / seconds
+
+
 def workload_name(nx, m, b):
     return f"NUFFT {nx}x{nx}, M={m}, {b}-problem lambda grid (8x8 log, 1e-4..1 of max|A^H y|)"
 
@@ -272,12 +289,8 @@ def run_ours(args):
         launches += L
     torch.cuda.synchronize()
     clk = clocks.stop()
-    total_ms = float(np.sum(ms_steps))
-    if world > 1:
-        tt = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
-    value = world * B * args.steps / (total_ms / 1e3)
+    total_ms = max_over_ranks([float(np.sum(ms_steps))], world, dist, dev)[0]
+    value = weak_rate(B * args.steps, world, total_ms / 1e3)
     other_prec = si.FP64 if chosen_prec == si.FP32 else si.FP32
     t = time.perf_counter()
     Xo, Ro = si.nufft_batch(*geo, probs, 0.0, precision=other_prec)
@@ -323,7 +336,8 @@ def run_ours(args):
         t = time.perf_counter()
         Xe, Re = si.nufft_batch(*h_geo, nx, nx, probs, 0.0, precision=chosen_prec)
         e2e_times.append(time.perf_counter() - t)
-    e2e_rate = world * B / float(np.mean(e2e_times))
+    e2e_s = max_over_ranks([float(np.mean(e2e_times))], world, dist, dev)[0]
+    e2e_rate = weak_rate(B, world, e2e_s)
     h2d = 5 * M * 8 + B * 48
     d2h = B * nx * nx * 8 + B * 144
 
