@@ -209,6 +209,11 @@ struct CtrlCfg {
   // still-active problem stops (device memory, set per solve)
   unsigned long long* steps;
   int refresh_every;  // > 0: FP32 form, refresh the FP64 anchor this often
+  // relative slack of the backtracking test F(xnew) <= Q (1 + slack): 0 for
+  // the FP64 forms (the reference's test); a rounding-level allowance for
+  // the corrected low-precision forms, whose F and Q come from differently
+  // rounded operator paths
+  double bt_slack;
 };
 
 // status codes written to ProbState.status (values of enum mfista_status)
@@ -294,7 +299,7 @@ __global__ void __launch_bounds__(128) k_control(const ProbParams* __restrict__ 
         s.active = 0;
         s.iters_out = s.iter + 1;
       } else {
-        bool finish = fval <= qval;
+        bool finish = fval <= qval + cfg.bt_slack * fabs(qval);
         if (!finish) {
           s.c *= kEta;
           s.trial += 1;

@@ -758,3 +758,96 @@ __global__ void __launch_bounds__(256, 2) k_nufft_spread_shared(NufftGeom<T> geo
 }
 
 }  // namespace mf
+
+// ===========================================================================
+// Forward model at the momentum point by linearity (corrected FP32 form).
+// MFISTA's momentum point is z = a x + b xnew with a, b set by the control
+// step (and x <- xnew when the trial improves the objective), so with the
+// models kept as visibility vectors ax = A x and axn = A xnew (written by
+// the trial point's forward pass), A z = a ax + b axn needs no NUFFT.
+// Vectors use the residual layout (problem b, point k at b y2_bstride + k).
+// ===========================================================================
+namespace mf {
+
+// weighted residual (vis - az) w^2 for the adjoint and its chi^2 partials.
+// The partials are summed in exactly the order of the interpolation kernel
+// that produces the same quantity for a trial point (k_nufft_interp_shared
+// with ppw points per warp, or k_nufft_interp with one point per warp), so
+// when the trial point equals z (a problem resting at x = 0, say) F(xnew)
+// and the f(z) inside Q agree to the bit and the backtracking test is not
+// decided by rounding.  Grid (chi slots, B), 256 threads.
+template <typename T>
+__global__ void k_nufft_resid_model(NufftGeom<T> geo, const double2* __restrict__ az, cplx<T>* __restrict__ y2,
+                                    int shared, int ppw, const ProbState* __restrict__ st, int gate, Partials part,
+                                    int qchi) {
+  __shared__ double sh[32];
+  __shared__ double s_chi[8];
+  const int b = blockIdx.y;
+  if (!gate_ok(st[b], gate)) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  auto term = [&](int k) {
+    const size_t e = (size_t)b * geo.y2_bstride + k;
+    const double2 m = az[e];
+    const double w = geo.weight[k];
+    const double rr = (geo.vis_r[k] - m.x) * w, ri = (geo.vis_i[k] - m.y) * w;
+    y2[e] = mk<T>((T)(rr * w), (T)(ri * w));
+    return rr * rr + ri * ri;
+  };
+  if (shared) {
+    // warp w: points (x * 8 + w) * ppw + q, q < ppw, summed in q order
+    const int mtot = geo.pt_hi[0];
+    const int kb = (blockIdx.x * 8 + warp) * ppw;
+    double t = 0.0;
+    if (lane < ppw && kb + lane < mtot) t = term(kb + lane);
+    double c = 0.0;
+    for (int q = 0; q < ppw; ++q) {
+      const double tq = __shfl_sync(0xffffffffu, t, q);
+      if (kb + q < mtot) c += tq;
+    }
+    if (lane == 0) s_chi[warp] = c;
+    __syncthreads();
+    if (threadIdx.x == 0 && qchi >= 0) {
+      double tot = 0.0;
+      for (int w = 0; w < 8; ++w) tot += s_chi[w];
+      part.at(qchi, b)[blockIdx.x] = tot;
+    }
+  } else {
+    // one point per warp, reduced over the CTA as k_nufft_interp does
+    const int k = geo.pt_lo[b] + blockIdx.x * 8 + warp;
+    double chi[1] = {0.0};
+    if (lane == 0 && k < geo.pt_hi[b]) chi[0] = term(k);
+    block_sum<1>(chi, sh);
+    if (threadIdx.x == 0 && qchi >= 0) part.at(qchi, b)[blockIdx.x] = chi[0];
+  }
+}
+
+// after the control step: az = mom_a ax + mom_b axn and ax = axn when the
+// trial point was taken (problems whose step was accepted)
+static __global__ void k_nufft_model_momentum(const int* __restrict__ pt_lo, const int* __restrict__ pt_hi, long bstride,
+                                       double2* __restrict__ ax, const double2* __restrict__ axn,
+                                       double2* __restrict__ az, const ProbState* __restrict__ st) {
+  const int b = blockIdx.y;
+  const ProbState& s = st[b];
+  if (!s.accepted) return;
+  const int k = pt_lo[b] + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= pt_hi[b]) return;
+  const size_t e = (size_t)b * bstride + k;
+  const double2 x = ax[e], xn = axn[e];
+  az[e] = make_double2(s.mom_a * x.x + s.mom_b * xn.x, s.mom_a * x.y + s.mom_b * xn.y);
+  if (s.take_x) ax[e] = xn;
+}
+
+// ax = src (and az = src when az is given) for the problems passing `gate`
+static __global__ void k_nufft_model_set(const int* __restrict__ pt_lo, const int* __restrict__ pt_hi, long bstride,
+                                  const double2* __restrict__ src, double2* __restrict__ ax,
+                                  double2* __restrict__ az, const ProbState* __restrict__ st, int gate) {
+  const int b = blockIdx.y;
+  if (!gate_ok(st[b], gate)) return;
+  const int k = pt_lo[b] + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= pt_hi[b]) return;
+  const size_t e = (size_t)b * bstride + k;
+  ax[e] = src[e];
+  if (az) az[e] = src[e];
+}
+
+}  // namespace mf

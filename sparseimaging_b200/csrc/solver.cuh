@@ -181,6 +181,13 @@ struct Op {
   virtual int device_error() { return 0; }
   // outer iterations between anchor refreshes of the corrected forms
   virtual int refresh_period() const { return 32; }
+  // forward model at the momentum point z by linearity from kept models of
+  // x and of the trial point (operators that keep them return true):
+  // forward_z replaces forward(z, ...) (residual kept, chi^2 into qchi),
+  // model_momentum follows k_momentum
+  virtual bool models_z() const { return false; }
+  virtual void forward_z(cudaStream_t s, int gate, int qchi) { (void)s; (void)gate; (void)qchi; }
+  virtual void model_momentum(cudaStream_t s) { (void)s; }
 };
 
 // ---------------------------------------------------------------------------
@@ -230,6 +237,8 @@ template <typename T> struct NufftOp : Op {
   bool shared;
   std::unique_ptr<NufftOp<double>> exact;  // FP64 operator for the anchors
   DevMem d_axa;                            // exact model of the anchors [y2 layout]
+  DevMem d_ax, d_axn, d_az;                // models of x, the trial point and z [y2 layout]
+  bool model = false;                      // forward at z by linearity (corrected form)
   DevMem d_u, d_v, d_mx, d_my, d_wx, d_wy, d_vr, d_vi, d_w, d_lo, d_hi, d_tptr, d_tpts, d_e4, d_grid, d_y2, tw2h;
   FftHost<T> fh, fcol;
   NufftGeom<T> geo{};
@@ -329,6 +338,14 @@ template <typename T> struct NufftOp : Op {
       exact.reset(new NufftOp<double>(ctx, in, false));
       exact->ippw = ippw;  // its chi^2 partials land in the same slots as ours
       d_axa.alloc(sizeof(double2) * (size_t)y2n);
+      const char* nm = getenv("MFISTA_NO_MODEL_Z");  // direct forward at z instead (comparison runs)
+      model = !(nm && nm[0] == '1');
+      if (model) {
+        for (DevMem* d : {&d_ax, &d_axn, &d_az}) {
+          d->alloc(sizeof(double2) * (size_t)y2n);
+          MF_CK(cudaMemset(d->p, 0, d->bytes));
+        }
+      }
       MF_CK(cudaMemset(d_axa.p, 0, d_axa.bytes));
     }
     geo.mx = d_mx.as<int>();
@@ -373,15 +390,38 @@ template <typename T> struct NufftOp : Op {
   }
 
   bool corrected() const override { return exact != nullptr; }
-  int launches_refresh() const override { return exact ? 3 : 0; }
+  int launches_refresh() const override { return exact ? (model ? 4 : 3) : 0; }
 
-  // exact FP64 model of the anchors: A x_a -> d_axa (owner's layout)
+  // exact FP64 model of the anchors: A x_a -> d_axa (owner's layout); the
+  // anchor is the current x, so its exact model also becomes the kept model
+  // of x (and of z at the start of a solve, where z = x)
   void refresh_anchor(cudaStream_t s, int gate) override {
     if (!exact) return;
     exact->launch_rows_fwd(s, c.xa, gate, nullptr);
     exact->launch_cols_fwd(s, gate);
     exact->launch_interp(s, exact->d_grid.template as<cplx<double>>(), gate, -1, nullptr, nullptr,
                          d_axa.as<double2>());
+    if (model) {
+      k_nufft_model_set<<<dim3(std::max(1, cdiv(mmax, 256)), B), 256, 0, s>>>(
+          geo.pt_lo, geo.pt_hi, geo.y2_bstride, d_axa.as<double2>(), d_ax.as<double2>(),
+          gate == kGateInit ? d_az.as<double2>() : nullptr, c.st, gate);
+      MF_LAUNCH_CK();
+    }
+  }
+
+  bool models_z() const override { return model; }
+
+  void forward_z(cudaStream_t s, int gate, int qchi) override {
+    k_nufft_resid_model<T><<<dim3(chi_slots(), B), 256, 0, s>>>(geo, d_az.as<double2>(), d_y2.as<cplx<T>>(),
+                                                                 shared ? 1 : 0, ippw, c.st, gate, c.part, qchi);
+    MF_LAUNCH_CK();
+  }
+
+  void model_momentum(cudaStream_t s) override {
+    if (!model) return;
+    k_nufft_model_momentum<<<dim3(std::max(1, cdiv(mmax, 256)), B), 256, 0, s>>>(
+        geo.pt_lo, geo.pt_hi, geo.y2_bstride, d_ax.as<double2>(), d_axn.as<double2>(), d_az.as<double2>(), c.st);
+    MF_LAUNCH_CK();
   }
 
   void forward_exact(cudaStream_t s, const double* src, int gate, int qchi, bool store) override {
@@ -425,7 +465,9 @@ template <typename T> struct NufftOp : Op {
     // with defect correction: A v = A x_a (FP64) + A32 (v - x_a)
     launch_rows_fwd(s, src, gate, exact ? c.xa : nullptr);
     launch_cols_fwd(s, gate);
-    launch_interp(s, g, gate, qchi, store ? d_y2.as<cplx<T>>() : nullptr, exact ? d_axa.as<double2>() : nullptr);
+    // the trial point's model is kept for the next momentum point
+    launch_interp(s, g, gate, qchi, store ? d_y2.as<cplx<T>>() : nullptr, exact ? d_axa.as<double2>() : nullptr,
+                  model && !store ? d_axn.as<double2>() : nullptr);
   }
 
   void adjoint(cudaStream_t s, const double* z_tsv, int qtsv) override {
@@ -1032,8 +1074,9 @@ struct Solver {
     refresh_every = op->corrected() ? op->refresh_period() : 0;
     if (const char* re = getenv("MFISTA_REFRESH_EVERY"))  // anchor refresh period (tuning)
       if (op->corrected() && atoi(re) > 0) refresh_every = atoi(re);
-    per_step_launches = op->launches_forward() * 2 + op->launches_adjoint() + 3 + (form == kFormTV ? 1 : 0) +
-                        (op->corrected() ? 1 + op->launches_refresh() : 0);
+    per_step_launches = op->launches_forward() * (op->models_z() ? 1 : 2) + op->launches_adjoint() + 3 +
+                        (form == kFormTV ? 1 : 0) + (op->corrected() ? 1 + op->launches_refresh() : 0) +
+                        (op->models_z() ? 2 : 0);
     fixed_launches = 2 * (op->launches_forward() + 2) + 1;
     const char* hl = getenv("MFISTA_HOST_LOOP");
     host_loop = hl && hl[0] == '1';
@@ -1153,6 +1196,7 @@ struct Solver {
     cfg.B = ctx.B;
     cfg.steps = d_steps.as<unsigned long long>();
     cfg.refresh_every = refresh_every;
+    cfg.bt_slack = refresh_every > 0 ? 1e-12 : 0.0;
     return cfg;
   }
 
@@ -1170,7 +1214,8 @@ struct Solver {
       op->refresh_anchor(s, kGateRefresh);
     }
     // gradient at z (only problems that start a new outer iteration)
-    op->forward(s, ctx.z, kGateGrad, kQChiZ, true);
+    if (op->models_z()) op->forward_z(s, kGateGrad, kQChiZ);
+    else op->forward(s, ctx.z, kGateGrad, kQChiZ, true);
     // the adjoint folds in the TSV gradient of z; TSV(z) itself is reduced by
     // k_update_tsv with the same tree as TSV(xnew)
     op->adjoint(s, form == kFormTSV ? ctx.z : nullptr, -1);
@@ -1187,6 +1232,7 @@ struct Solver {
     launch_control(s, kCtrlStep, h, set_handle);
     k_momentum<<<ig, 256, 0, s>>>(ctx.x, ctx.z, ctx.xnew, dm, ctx.st);
     MF_LAUNCH_CK();
+    op->model_momentum(s);
   }
 
   void drop_graphs() {
