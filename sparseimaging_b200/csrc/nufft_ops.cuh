@@ -584,21 +584,73 @@ __global__ void __launch_bounds__(256, SharedChunk<T>::kInterpMinBlocks) k_nufft
 // broadcasts, so a point that misses a cell costs one mask test.
 constexpr int kSpreadTile = 16;
 
-// shared-memory staging of one CTA of the spreading kernel
+// asynchronous global -> shared copies (cp.async): 4, 8 or 16 bytes
+__device__ __forceinline__ void cp_async(void* smem_dst, const void* gmem_src, int bytes) {
+  const unsigned int d = (unsigned int)__cvta_generic_to_shared(smem_dst);
+  if (bytes == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+  else if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem_src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// shared-memory staging of one CTA of the spreading kernel: two buffers, so
+// the points of the next round are copied in while this round is summed
 template <typename T, int PB> struct SpreadSmem {
   static constexpr int P = 32;  // points staged per round
-  int ox[P], oy[P];             // 11 - mx, 11 - my
-  unsigned int mask[P];         // rows (low 16 bits) | cols (high 16 bits)
-  T wx[P][kTaps], wy[P][kTaps];
-  __align__(16) cplx<T> r[P][PB];
+  struct Buf {
+    __align__(16) T wx[P][kTaps];
+    __align__(16) T wy[P][kTaps];
+    __align__(16) cplx<T> r[P][PB];
+    int mx[P], my[P];
+  } buf[2];
   int list[PB];                 // the chunk's active problems, compacted
   int cnt;
 };
+
+// issues the copies of points [c0, c0 + np) of the tile's list into b:
+// their grid indices, 24 + 24 tap weights (16-byte pieces) and the first
+// NB slots' residuals (zero for slots >= cnt)
+template <typename T, int PB, int NB>
+__device__ __forceinline__ void spread_stage(const NufftGeom<T>& geo, const cplx<T>* __restrict__ y2, int c0, int np,
+                                             int b0, int cnt, SpreadSmem<T, PB>& sm,
+                                             typename SpreadSmem<T, PB>::Buf& b) {
+  constexpr int kPieces = kTaps * sizeof(T) / 16;  // 16-byte pieces per point and axis
+  for (int t = threadIdx.x; t < np; t += blockDim.x) {
+    const int k = geo.tile_pts[c0 + t];
+    cp_async(&b.mx[t], geo.mx + k, 4);
+    cp_async(&b.my[t], geo.my + k, 4);
+  }
+  for (int t = threadIdx.x; t < np * 2 * kPieces; t += blockDim.x) {
+    const int pp = t / (2 * kPieces), r = t - pp * 2 * kPieces;
+    const int axis = r / kPieces, piece = r - axis * kPieces;
+    const int k = geo.tile_pts[c0 + pp];
+    const T* src = (axis ? geo.wy : geo.wx) + (size_t)k * kTaps + piece * (16 / sizeof(T));
+    T* dst = (axis ? &b.wy[pp][0] : &b.wx[pp][0]) + piece * (16 / sizeof(T));
+    cp_async(dst, src, 16);
+  }
+  for (int t = threadIdx.x; t < np * NB; t += blockDim.x) {
+    const int pp = t / NB, i = t - pp * NB;
+    if (i < cnt) {
+      const int k = geo.tile_pts[c0 + pp];
+      cp_async(&b.r[pp][i], y2 + (size_t)(b0 + sm.list[i]) * geo.y2_bstride + k, (int)sizeof(cplx<T>));
+    } else {
+      b.r[pp][i] = mk<T>(0, 0);
+    }
+  }
+}
 
 // Accumulates the tile's segment of points for the first NB active problems
 // of the chunk (NB >= cnt) and writes the cluster's sum.  NB is a compile-time
 // bound so that a chunk with few active problems (the tail of a lambda grid)
 // runs a short FMA loop while a full chunk keeps a fully unrolled one.
+// Points come in rounds of P through the two shared buffers: the copies of
+// round r + 1 (cp.async) are in flight while round r is summed.
 template <typename T, int PB, int NB>
 __device__ __forceinline__ void spread_tile(const NufftGeom<T>& geo, const cplx<T>* __restrict__ y2,
                                             cplx<T>* __restrict__ gall, long gstride, int nx, int ny, int tile,
@@ -609,8 +661,7 @@ __device__ __forceinline__ void spread_tile(const NufftGeom<T>& geo, const cplx<
   const int ntc = (ny + 1 + TILE - 1) / TILE;
   const int tr = tile / ntc, tc = tile - tr * ntc;
   const int ty = threadIdx.x / TILE, tx = threadIdx.x - ty * TILE;
-  const int row0 = tr * TILE, col0 = tc * TILE;
-  const int row = row0 + ty, col = col0 + tx;
+  const int row = tr * TILE + ty, col = tc * TILE + tx;
   const bool valid = row < 2 * nx && col <= ny;
   const int mrow = row < nx ? row : row - 2 * nx;
   const int mcol = col < ny ? col : -ny;
@@ -620,58 +671,21 @@ __device__ __forceinline__ void spread_tile(const NufftGeom<T>& geo, const cplx<
   const int lbeg = geo.tile_ptr[tile], lend = geo.tile_ptr[tile + 1];
   const int seg = (lend - lbeg + csize - 1) / csize;
   const int beg = min(lend, lbeg + rank * seg), end = min(lend, beg + seg);
-  for (int c0 = beg; c0 < end; c0 += P) {
+  const int rounds = (end - beg + P - 1) / P;
+  if (rounds > 0) spread_stage<T, PB, NB>(geo, y2, beg, min(P, end - beg), b0, cnt, sm, sm.buf[0]);
+  cp_async_commit();
+  for (int rd = 0; rd < rounds; ++rd) {
+    const int c0 = beg + rd * P;
     const int np = min(P, end - c0);
-    __syncthreads();
-    {
-      // tile rows / columns reached by each point's direct or mirrored
-      // footprint: warp w takes points w, w + 8, ...; lane q < 16 tests tile
-      // row q, lane 16 + q tile column q, and one ballot gives the mask
-      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-      const int q = lane & (TILE - 1);
-      const int r = row0 + q, cc = col0 + q;
-      const int mr = r < nx ? r : r - 2 * nx;
-      const int mc = cc < ny ? cc : -ny;
-      for (int t = warp; t < np; t += 8) {
-        const int k = geo.tile_pts[c0 + t];
-        const int mx = geo.mx[k], my = geo.my[k];
-        bool hit;
-        if (lane < TILE)
-          hit = r < 2 * nx && ((unsigned)(mr - mx + (kMSP - 1)) < (unsigned)kTaps ||
-                               (unsigned)(-mr - mx + (kMSP - 1)) < (unsigned)kTaps);
-        else
-          hit = cc <= ny && ((unsigned)(mc - my + (kMSP - 1)) < (unsigned)kTaps ||
-                             (unsigned)(-mc - my + (kMSP - 1)) < (unsigned)kTaps);
-        const unsigned int m = __ballot_sync(0xffffffffu, hit);
-        if (lane == 0) {
-          sm.ox[t] = (kMSP - 1) - mx;
-          sm.oy[t] = (kMSP - 1) - my;
-          sm.mask[t] = m;
-        }
-      }
-    }
-    for (int t = threadIdx.x; t < np * kTaps; t += blockDim.x) {
-      int pp = t / kTaps, j = t - pp * kTaps;
-      int k = geo.tile_pts[c0 + pp];
-      sm.wx[pp][j] = geo.wx[(size_t)k * kTaps + j];
-      sm.wy[pp][j] = geo.wy[(size_t)k * kTaps + j];
-    }
-    for (int t = threadIdx.x; t < np * NB; t += blockDim.x) {
-      int pp = t / NB, i = t - pp * NB;
-      int k = geo.tile_pts[c0 + pp];
-      cplx<T> r = mk<T>(0, 0);
-      if (i < cnt) {
-        r = y2[(size_t)(b0 + sm.list[i]) * geo.y2_bstride + k];
-        r.y = -r.y;  // NU_SIGN * Fin_i
-      }
-      sm.r[pp][i] = r;
-    }
-    __syncthreads();
+    if (rd + 1 < rounds)
+      spread_stage<T, PB, NB>(geo, y2, c0 + P, min(P, end - c0 - P), b0, cnt, sm, sm.buf[(rd + 1) & 1]);
+    cp_async_commit();
+    cp_async_wait<1>();  // this thread's copies of round rd have landed
+    __syncthreads();     // and everyone's
+    const typename SpreadSmem<T, PB>::Buf& b = sm.buf[rd & 1];
     if (valid) {
-      const unsigned int mybits = (1u << ty) | (1u << (16 + tx));
       for (int pp = 0; pp < np; ++pp) {
-        if ((sm.mask[pp] & mybits) != mybits) continue;
-        const int ox = sm.ox[pp], oy = sm.oy[pp];
+        const int ox = (kMSP - 1) - b.mx[pp], oy = (kMSP - 1) - b.my[pp];
         const int lxd = mrow + ox, lyd = mcol + oy;
         const int lxm = ox - mrow, lym = oy - mcol;
         const bool d = (unsigned)lxd < (unsigned)kTaps && (unsigned)lyd < (unsigned)kTaps;
@@ -683,18 +697,21 @@ __device__ __forceinline__ void spread_tile(const NufftGeom<T>& geo, const cplx<
           const bool use_m = (pass == 0) ? mfirst : (mi && !mfirst);
           const bool use_d = (pass == 0) ? (d && !mfirst) : (d && mfirst);
           if (!(use_m || use_d)) continue;
-          const T w = use_m ? sm.wy[pp][lym] * sm.wx[pp][lxm] : sm.wy[pp][lyd] * sm.wx[pp][lxd];
+          const T w = use_m ? b.wy[pp][lym] * b.wx[pp][lxm] : b.wy[pp][lyd] * b.wx[pp][lxd];
           const T hw = w * T(0.5);
-          const T hwi = use_m ? -hw : hw;
+          // the staged residual keeps its sign; NU_SIGN on Fin_i is folded
+          // into the imaginary weight (exact: (-a) b == a (-b))
+          const T hwi = use_m ? hw : -hw;
 #pragma unroll
           for (int i = 0; i < NB; ++i) {
-            cplx<T> r = sm.r[pp][i];
+            cplx<T> r = b.r[pp][i];
             ar[i] += r.x * hw;
             ai[i] += r.y * hwi;
           }
         }
       }
     }
+    __syncthreads();  // buffer rd & 1 is refilled by the copies issued in the next round
   }
   // segment accumulators -> shared memory; rank 0 adds ranks 1.. in order
 #pragma unroll
