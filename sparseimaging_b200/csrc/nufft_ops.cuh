@@ -457,12 +457,14 @@ template <> struct SharedChunk<float> {
   static constexpr int kSpread = 16;  // problems per spreading CTA
   static constexpr int kInterpMinBlocks = 2;
   static constexpr int kInterpPts = 2;  // default points per warp
+  static constexpr int kSpreadMinBlocks = 3;
 };
 template <> struct SharedChunk<double> {
   static constexpr int kInterp = 8;
   static constexpr int kSpread = 8;
   static constexpr int kInterpMinBlocks = 2;
   static constexpr int kInterpPts = 8;
+  static constexpr int kSpreadMinBlocks = 3;
 };
 
 // interpolation: one warp per point, lanes over the 576 taps (18 each) with
@@ -737,7 +739,7 @@ __device__ __forceinline__ void spread_tile(const NufftGeom<T>& geo, const cplx<
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256, 2) k_nufft_spread_shared(NufftGeom<T> geo, const cplx<T>* __restrict__ y2,
+__global__ void __launch_bounds__(256, SharedChunk<T>::kSpreadMinBlocks) k_nufft_spread_shared(NufftGeom<T> geo, const cplx<T>* __restrict__ y2,
                                                                 cplx<T>* __restrict__ gall, long gstride, int nx,
                                                                 int ny, int ntiles, const ProbState* __restrict__ st,
                                                                 int gate, int B) {
