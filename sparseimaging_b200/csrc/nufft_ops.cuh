@@ -455,7 +455,7 @@ template <typename T> struct SharedChunk;
 template <> struct SharedChunk<float> {
   static constexpr int kInterp = 16;  // problems per interpolation CTA
   static constexpr int kSpread = 16;  // problems per spreading CTA
-  static constexpr int kInterpMinBlocks = 2;
+  static constexpr int kInterpMinBlocks = 3;
   static constexpr int kInterpPts = 2;  // default points per warp
   static constexpr int kSpreadMinBlocks = 3;
 };
