@@ -794,13 +794,18 @@ namespace mf {
 // with ppw points per warp, or k_nufft_interp with one point per warp), so
 // when the trial point equals z (a problem resting at x = 0, say) F(xnew)
 // and the f(z) inside Q agree to the bit and the backtracking test is not
-// decided by rounding.  Grid (chi slots, B), 256 threads.
+// decided by rounding.  Grid (cdiv(chi slots, 8), B) for shared geometry
+// (one warp per slot), (chi slots, B) otherwise; 256 threads.
+template <typename T> __device__ __forceinline__ int slots_of(const NufftGeom<T>& geo, int ppw) {
+  const int m = geo.pt_hi[0];
+  return max(1, (m + 8 * ppw - 1) / (8 * ppw));
+}
+
 template <typename T>
 __global__ void k_nufft_resid_model(NufftGeom<T> geo, const double2* __restrict__ az, cplx<T>* __restrict__ y2,
                                     int shared, int ppw, const ProbState* __restrict__ st, int gate, Partials part,
                                     int qchi) {
   __shared__ double sh[32];
-  __shared__ double s_chi[8];
   const int b = blockIdx.y;
   if (!gate_ok(st[b], gate)) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -813,22 +818,25 @@ __global__ void k_nufft_resid_model(NufftGeom<T> geo, const double2* __restrict_
     return rr * rr + ri * ri;
   };
   if (shared) {
-    // warp w: points (x * 8 + w) * ppw + q, q < ppw, summed in q order
+    // one warp per slot (a CTA of the interpolation: 8 warps x ppw points);
+    // the terms go through shared memory and lane 0 adds them in the
+    // interpolation's order (per warp w in q order, then over w)
+    __shared__ double s_t[8][8 * 32];
+    const int slot = blockIdx.x * 8 + warp;
+    if (slot >= slots_of(geo, ppw)) return;
     const int mtot = geo.pt_hi[0];
-    const int kb = (blockIdx.x * 8 + warp) * ppw;
-    double t = 0.0;
-    if (lane < ppw && kb + lane < mtot) t = term(kb + lane);
-    double c = 0.0;
-    for (int q = 0; q < ppw; ++q) {
-      const double tq = __shfl_sync(0xffffffffu, t, q);
-      if (kb + q < mtot) c += tq;
-    }
-    if (lane == 0) s_chi[warp] = c;
-    __syncthreads();
-    if (threadIdx.x == 0 && qchi >= 0) {
+    const int n = 8 * ppw, k0 = slot * n;
+    for (int l = lane; l < n; l += 32) s_t[warp][l] = (k0 + l < mtot) ? term(k0 + l) : 0.0;
+    __syncwarp();
+    if (lane == 0 && qchi >= 0) {
       double tot = 0.0;
-      for (int w = 0; w < 8; ++w) tot += s_chi[w];
-      part.at(qchi, b)[blockIdx.x] = tot;
+      for (int w = 0; w < 8; ++w) {
+        double c = 0.0;
+        for (int q = 0; q < ppw; ++q)
+          if (k0 + w * ppw + q < mtot) c += s_t[warp][w * ppw + q];
+        tot += c;
+      }
+      part.at(qchi, b)[slot] = tot;
     }
   } else {
     // one point per warp, reduced over the CTA as k_nufft_interp does

@@ -412,8 +412,9 @@ template <typename T> struct NufftOp : Op {
   bool models_z() const override { return model; }
 
   void forward_z(cudaStream_t s, int gate, int qchi) override {
-    k_nufft_resid_model<T><<<dim3(chi_slots(), B), 256, 0, s>>>(geo, d_az.as<double2>(), d_y2.as<cplx<T>>(),
-                                                                 shared ? 1 : 0, ippw, c.st, gate, c.part, qchi);
+    const int gx = shared ? cdiv(chi_slots(), 8) : chi_slots();
+    k_nufft_resid_model<T><<<dim3(gx, B), 256, 0, s>>>(geo, d_az.as<double2>(), d_y2.as<cplx<T>>(), shared ? 1 : 0,
+                                                        ippw, c.st, gate, c.part, qchi);
     MF_LAUNCH_CK();
   }
 
