@@ -188,6 +188,24 @@ def config0(seed=0):
     return nufft_problem(64, 8, 72, seed)
 
 
+def movie_problem(n_frames=48, nx=128, seed=3, m_range=(800, 12000), noise_frac=0.02):
+    """Frames of a movie with uneven visibility counts: frame f shows
+    sky_movie_frame(nx, f) (the ring's bright spot turns 7.5 degrees per
+    frame, two static blobs); its uv coverage has 6-10 stations and as many
+    hour angles over 12 h as bring M = baselines x hours near a value drawn
+    uniformly from m_range.  Noise: noise_frac of max|V| per frame."""
+    rng = np.random.default_rng(seed)
+    frames = []
+    for f in range(n_frames):
+        ns = int(rng.integers(6, 11))
+        nb = ns * (ns - 1) // 2
+        m_goal = rng.uniform(*m_range)
+        nh = max(1, int(round(m_goal / nb)))
+        sky = sky_movie_frame(nx, f, seed=seed)
+        frames.append(nufft_problem(nx, ns, nh, int(rng.integers(1 << 30)), noise_frac=noise_frac, sky=sky))
+    return frames
+
+
 def lambda_grid_problem(seed=7, nx=128, n_stations=10, n_hours=180):
     """128x128 NUFFT problem (M = 45 * 180 = 8100) shared by a lambda grid."""
     return nufft_problem(nx, n_stations, n_hours, seed)
