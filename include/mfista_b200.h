@@ -203,10 +203,13 @@ int mfista_plan_get_shapes(mfista_plan plan, int *shapes);
 int mfista_plan_set_shapes(mfista_plan plan, const int *shapes);
 /* Autotuner: times every candidate shape of each knob above with the
  * plan's kernels in isolation (as mfista_plan_profile, `reps` launches),
- * one knob at a time, keeps the fastest, and captures the graph again.
- * shapes_out: int[4] chosen shapes; ms_out: double[4] best time per launch
- * of each knob's kernels (0 for unused knobs).  Either may be NULL.  Like
- * mfista_plan_profile, it leaves the iterates undefined. */
+ * one knob at a time, both with every problem active (t_all) and with one
+ * problem active (t_one, the tail of a batched solve), keeps the shape
+ * minimising t_all / min t_all + t_one / min t_one, and captures the graph
+ * again.  shapes_out: int[4] chosen shapes; ms_out: double[4] t_all per
+ * launch of each knob's kernels at the chosen shape (0 for unused knobs).
+ * Either may be NULL.  Like mfista_plan_profile, it leaves the iterates
+ * undefined. */
 int mfista_plan_tune(mfista_plan plan, int reps, int *shapes_out, double *ms_out);
 /* Per-problem status of the last fetched solve (enum mfista_status values). */
 int mfista_plan_statuses(mfista_plan plan, int *status_out);

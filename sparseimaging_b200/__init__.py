@@ -425,9 +425,11 @@ class Plan:
         _check(lib().mfista_plan_set_shapes(self.h, a))
 
     def tune(self, reps=10):
-        """Autotunes the launch shapes on this GPU; returns (shapes, best ms
-        per launch of each knob's kernels).  Iterates are left undefined:
-        call set_problems before the next run."""
+        """Autotunes the launch shapes on this GPU (scoring each candidate
+        on the whole batch and on one active problem); returns (shapes, ms
+        per launch of each knob's kernels at the chosen shape, whole batch
+        active).  Iterates are left undefined: call set_problems before the
+        next run."""
         a = (C.c_int * 4)()
         ms = np.zeros(4)
         _check(lib().mfista_plan_tune(self.h, reps, a, _p(ms)))

@@ -112,6 +112,39 @@ __device__ __forceinline__ bool gate_ok(const ProbState& s, int gate) {
   }
 }
 
+// Problem chunks over the batch's active problems: the problems passing
+// `gate`, in index order, are cut into chunks of PB; chunk `chunk` gets
+// ranks [chunk PB, chunk PB + PB).  Writes that chunk's problem indices to
+// list[] and returns their count (0: nothing to do).  Every CTA of a launch
+// sees the same ranking, so a problem lands in exactly one chunk however
+// the active problems are spread over the batch.  Called by all threads of
+// a 256-thread CTA; s_cnt is 8 ints of shared memory.
+template <int PB>
+__device__ __forceinline__ int active_chunk(const ProbState* __restrict__ st, int gate, int B, int chunk, int* list,
+                                            int* s_cnt) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int lo = chunk * PB;
+  int base_rank = 0;
+  for (int base = 0; base < B; base += 256) {
+    const int b = base + (int)threadIdx.x;
+    const bool on = b < B && gate_ok(st[b], gate);
+    const unsigned int bal = __ballot_sync(0xffffffffu, on);
+    if (lane == 0) s_cnt[warp] = __popc(bal);
+    __syncthreads();
+    int r = base_rank + __popc(bal & ((1u << lane) - 1u)), tot = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+      const int c = s_cnt[w];
+      if (w < warp) r += c;
+      tot += c;
+    }
+    if (on && r >= lo && r < lo + PB) list[r - lo] = b;
+    base_rank += tot;
+    __syncthreads();  // s_cnt is rewritten by the next round
+  }
+  return min(max(base_rank - lo, 0), PB);
+}
+
 // deterministic reductions --------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

@@ -471,9 +471,10 @@ template <> struct SharedChunk<double> {
 // cell and weight held in registers, looping over the CTA's problem chunk;
 // each warp takes `ppw` consecutive points (a launch-shape choice: the
 // per-point arithmetic does not depend on it, the grouping of the chi^2
-// partial sums does)
+// partial sums does).  kActiveChunks: chunk y holds the y-th PB of the
+// batch's active problems (active_chunk) instead of problems [y PB, y PB + PB).
 
-template <typename T>
+template <typename T, bool kActiveChunks = false>
 __global__ void __launch_bounds__(256, SharedChunk<T>::kInterpMinBlocks) k_nufft_interp_shared(NufftGeom<T> geo, const cplx<T>* __restrict__ gall,
                                                              long gstride, int nx, int ny, double inv_mm,
                                                              const ProbState* __restrict__ st, int gate,
@@ -484,9 +485,14 @@ __global__ void __launch_bounds__(256, SharedChunk<T>::kInterpMinBlocks) k_nufft
   constexpr int NT = (kTaps * kTaps) / 32;
   __shared__ double s_chi[8][PB];
   __shared__ int s_act[PB];
-  const int b0 = blockIdx.y * PB;
-  if (threadIdx.x < PB) {
-    int b = b0 + threadIdx.x;
+  __shared__ int s_prob[PB];  // problem of chunk slot i
+  if (kActiveChunks) {
+    __shared__ int s_cnt[8];
+    const int n = active_chunk<PB>(st, gate, B, blockIdx.y, s_prob, s_cnt);
+    if (threadIdx.x < PB) s_act[threadIdx.x] = threadIdx.x < n ? 1 : 0;
+  } else if (threadIdx.x < PB) {
+    const int b = blockIdx.y * PB + threadIdx.x;
+    s_prob[threadIdx.x] = b;
     s_act[threadIdx.x] = (b < B && gate_ok(st[b], gate)) ? 1 : 0;
   }
   __syncthreads();
@@ -533,7 +539,7 @@ __global__ void __launch_bounds__(256, SharedChunk<T>::kInterpMinBlocks) k_nufft
 #pragma unroll 1
     for (int i = 0; i < PB; ++i) {
       if (!s_act[i]) continue;
-      const int b = b0 + i;
+      const int b = s_prob[i];
       const cplx<T>* g = gall + (size_t)b * gstride;
       T accr = 0, acci = 0;
 #pragma unroll
@@ -571,7 +577,206 @@ __global__ void __launch_bounds__(256, SharedChunk<T>::kInterpMinBlocks) k_nufft
     double c = 0.0;
 #pragma unroll
     for (int w = 0; w < 8; ++w) c += s_chi[w][threadIdx.x];
-    part.at(qchi, b0 + threadIdx.x)[blockIdx.x] = c;
+    part.at(qchi, s_prob[threadIdx.x])[blockIdx.x] = c;
+  }
+}
+
+// Grouped interpolation: the same warp-per-point tap layout as
+// k_nufft_interp_shared, but the CTA's active problems (compacted into a
+// list) are taken G at a time with the G accumulator pairs held together,
+// so the tap loop issues G independent loads per tap and each tap's address
+// and weight serve G problems; G is 8, 4, 2 or 1 as the number of remaining
+// active problems allows (FP32 only: 2G double sums do not fit the register
+// budget, and FP64 plans use k_nufft_interp_shared).  Points whose 576 taps are all
+// direct and inside the grid (the usual case; warp-uniform) take a loop
+// without per-tap flag tests that adds the same products in the same order
+// as the general loop.  The 2G sums are reduced over the warp by a
+// transposing butterfly: at each of the first log2(2G) levels a lane keeps
+// half of its values and receives the partner's copy of that half, so
+// 2G - 1 shuffles (plus 5 - log2(2G) plain levels) leave lane L with value
+// L >> (5 - log2(2G)); real parts sit in lanes 0-15, imaginary parts in
+// lanes 16-31, and one lane per problem finishes the G problems in
+// parallel.  Each level adds a lane's partial to that of lane L ^ off, the
+// same pairs in the same order as the plain butterfly (offsets 16, 8, 4, 2,
+// 1) of k_nufft_interp_shared, so a point's value does not depend on G and
+// equals that kernel's to the bit.  Partial chi^2 sums are kept per (warp,
+// problem) in point order, as in k_nufft_interp_shared.
+template <typename T> struct GroupChunk;
+template <> struct GroupChunk<float> {
+  static constexpr int kGmax = 8;  // 16 float sums per lane
+  static constexpr int kMinBlocks = 2;
+};
+
+// transposing warp reduction of 2^V values (V <= 5): afterwards every lane
+// holds the warp-wide sum of value (lane >> (5 - V)) in v[0]
+template <int V, typename T> __device__ __forceinline__ void transpose_reduce(T (&v)[1 << V], int lane) {
+#pragma unroll
+  for (int lvl = 0; lvl < V; ++lvl) {
+    const int half = (1 << V) >> (lvl + 1);  // values kept after this level
+    const int off = 16 >> lvl;
+    const bool upper = (lane & off) != 0;
+#pragma unroll
+    for (int j = 0; j < half; ++j) {
+      const T send = upper ? v[j] : v[j + half];
+      const T keep = upper ? v[j + half] : v[j];
+      v[j] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+    }
+  }
+#pragma unroll
+  for (int off = 16 >> V; off > 0; off >>= 1) v[0] += __shfl_xor_sync(0xffffffffu, v[0], off);
+}
+
+// per-point data of one interpolation pass
+template <typename T> struct InterpPoint {
+  static constexpr int NT = (kTaps * kTaps) / 32;
+  int cell[NT];  // grid index | mirrored << 30, or -1
+  T wgt[NT];
+  bool plain;    // every tap of the warp direct and inside the grid
+  int k;
+  double w, vr, vi;
+};
+
+// G problems of the CTA's active list starting at list[pos]
+template <typename T, int G>
+__device__ __forceinline__ void interp_group(const InterpPoint<T>& P, const cplx<T>* __restrict__ gall, long gstride,
+                                             const int* list, int pos, int lane, double inv_mm,
+                                             const NufftGeom<T>& geo, const double2* __restrict__ ax_base,
+                                             double2* __restrict__ ax_out, cplx<T>* __restrict__ y2,
+                                             double* s_chi_w) {
+  constexpr int V = (G == 8) ? 4 : (G == 4) ? 3 : (G == 2) ? 2 : 1;  // 2G = 2^V sums
+  constexpr int NT = InterpPoint<T>::NT;
+  const cplx<T>* g[G];
+#pragma unroll
+  for (int i = 0; i < G; ++i) g[i] = gall + (size_t)list[pos + i] * gstride;
+  T acc[2 * G];
+#pragma unroll
+  for (int i = 0; i < 2 * G; ++i) acc[i] = 0;
+  if (P.plain) {
+#pragma unroll
+    for (int s = 0; s < NT; ++s) {
+      const int cc = P.cell[s];
+#pragma unroll
+      for (int i = 0; i < G; ++i) {
+        const cplx<T> gv = g[i][cc];
+        acc[i] += gv.x * P.wgt[s];
+        acc[G + i] += (-gv.y) * P.wgt[s];  // NU_SIGN: direct taps only
+      }
+    }
+  } else {
+#pragma unroll
+    for (int s = 0; s < NT; ++s) {
+      const int cc = P.cell[s];
+      if (cc >= 0) {
+        const bool mir = (cc >> 30) != 0;
+#pragma unroll
+        for (int i = 0; i < G; ++i) {
+          const cplx<T> gv = g[i][cc & 0x3fffffff];
+          acc[i] += gv.x * P.wgt[s];
+          // NU_SIGN on the imaginary part of direct taps, + on mirrored ones
+          acc[G + i] += (mir ? gv.y : -gv.y) * P.wgt[s];
+        }
+      }
+    }
+  }
+  transpose_reduce<V>(acc, lane);
+  const T im = __shfl_xor_sync(0xffffffffu, acc[0], 16);
+  const int fin = lane >> (5 - V);
+  if (lane < 16 && (lane & ((1 << (5 - V)) - 1)) == 0) {
+    const int slot = pos + fin;
+    const int b = list[slot];
+    double fr = (double)acc[0] * inv_mm, fi = (double)im * inv_mm;
+    const size_t e = (size_t)b * geo.y2_bstride + P.k;
+    if (ax_base) {
+      fr += ax_base[e].x;
+      fi += ax_base[e].y;
+    }
+    if (ax_out) ax_out[e] = make_double2(fr, fi);
+    const double rr = (P.vr - fr) * P.w;
+    const double ri = (P.vi - fi) * P.w;
+    s_chi_w[slot] += rr * rr + ri * ri;
+    if (y2) y2[e] = mk<T>((T)(rr * P.w), (T)(ri * P.w));
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, GroupChunk<T>::kMinBlocks) k_nufft_interp_group(
+    NufftGeom<T> geo, const cplx<T>* __restrict__ gall, long gstride, int nx, int ny, double inv_mm,
+    const ProbState* __restrict__ st, int gate, Partials part, int qchi, cplx<T>* __restrict__ y2, int B,
+    const double2* __restrict__ ax_base, double2* __restrict__ ax_out, int ppw) {
+  constexpr int PB = SharedChunk<T>::kInterp;
+  constexpr int GM = GroupChunk<T>::kGmax;
+  constexpr int NT = InterpPoint<T>::NT;
+  __shared__ double s_chi[8][PB];  // per warp, per list slot
+  __shared__ int s_list[PB];
+  __shared__ int s_cnt[8];
+  const int nact = active_chunk<PB>(st, gate, B, blockIdx.y, s_list, s_cnt);
+  if (nact == 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int mtot = geo.pt_hi[0];
+  if (lane < PB) s_chi[warp][lane] = 0.0;
+  __syncwarp();
+  for (int q = 0; q < ppw; ++q) {
+    InterpPoint<T> P;
+    P.k = (blockIdx.x * 8 + warp) * ppw + q;
+    if (P.k >= mtot) break;
+    const int k = P.k;
+    bool plain = true;
+    const int mxk = geo.mx[k], myk = geo.my[k];
+    const T* wxk = geo.wx + (size_t)k * kTaps;
+    const T* wyk = geo.wy + (size_t)k * kTaps;
+#pragma unroll
+    for (int s = 0; s < NT; ++s) {
+      const int t = lane + 32 * s;
+      const int lx = t / kTaps, ly = t - lx * kTaps;
+      const int m = myk + ly - (kMSP - 1);
+      const int mxm = mxk + lx - (kMSP - 1);
+      int col = half_col(m, ny), row, mirror = 0;
+      if (col >= 0) {
+        row = wrap_row(mxm, nx);
+      } else {
+        col = half_col(-m, ny);
+        row = wrap_row(-mxm, nx);
+        mirror = 1;
+      }
+      if (col >= 0 && row >= 0) {
+        P.cell[s] = (row * (ny + 1) + col) | (mirror << 30);
+        P.wgt[s] = wyk[ly] * wxk[lx];
+        plain = plain && !mirror;
+      } else {
+        P.cell[s] = -1;
+        P.wgt[s] = 0;
+        plain = false;
+      }
+    }
+    P.plain = __all_sync(0xffffffffu, plain);
+    P.w = geo.weight[k];
+    P.vr = geo.vis_r[k];
+    P.vi = geo.vis_i[k];
+    int pos = 0;
+    while (pos < nact) {
+      const int rem = nact - pos;
+      if (GM >= 8 && rem >= 8) {
+        interp_group<T, (GM >= 8 ? 8 : 1)>(P, gall, gstride, s_list, pos, lane, inv_mm, geo, ax_base, ax_out,
+                                           y2, s_chi[warp]);
+        pos += 8;
+      } else if (GM >= 4 && rem >= 4) {
+        interp_group<T, (GM >= 4 ? 4 : 1)>(P, gall, gstride, s_list, pos, lane, inv_mm, geo, ax_base, ax_out, y2, s_chi[warp]);
+        pos += 4;
+      } else if (rem >= 2) {
+        interp_group<T, 2>(P, gall, gstride, s_list, pos, lane, inv_mm, geo, ax_base, ax_out, y2, s_chi[warp]);
+        pos += 2;
+      } else {
+        interp_group<T, 1>(P, gall, gstride, s_list, pos, lane, inv_mm, geo, ax_base, ax_out, y2, s_chi[warp]);
+        pos += 1;
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < nact && qchi >= 0) {
+    double c = 0.0;
+#pragma unroll
+    for (int wp = 0; wp < 8; ++wp) c += s_chi[wp][threadIdx.x];
+    part.at(qchi, s_list[threadIdx.x])[blockIdx.x] = c;
   }
 }
 
@@ -752,18 +957,11 @@ __global__ void __launch_bounds__(256, SharedChunk<T>::kSpreadMinBlocks) k_nufft
   cg::cluster_group cluster = cg::this_cluster();
   const int rank = (int)cluster.block_rank();
   const int csize = (int)cluster.num_blocks();
-  const int b0 = blockIdx.y * PB;
-  if (threadIdx.x == 0) {
-    int n = 0;
-    for (int i = 0; i < PB; ++i) {
-      int b = b0 + i;
-      if (b < B && gate_ok(st[b], gate)) sm.list[n++] = i;
-    }
-    sm.cnt = n;
-  }
-  __syncthreads();
-  const int cnt = sm.cnt;
+  // chunks over the batch's active problems (list: problem indices)
+  __shared__ int s_cnt[8];
+  const int cnt = active_chunk<PB>(st, gate, B, blockIdx.y, sm.list, s_cnt);
   if (cnt == 0) return;  // uniform over the cluster: same problem chunk
+  const int b0 = 0;
   const int tile = blockIdx.x / csize;
   // accumulator slot i holds problem b0 + list[i]: the smallest unrolled
   // width that holds the chunk's active problems

@@ -373,10 +373,16 @@ template <typename T> struct NufftOp : Op {
 
   void launch_interp(cudaStream_t s, cplx<T>* g, int gate, int qchi, cplx<T>* y2, const double2* base = nullptr,
                      double2* out = nullptr) {
-    if (shared)
-      k_nufft_interp_shared<T><<<dim3(interp_blocks(), interp_chunks()), 256, 0, s>>>(
-          geo, g, gstride, nx, ny, inv_mm, c.st, gate, c.part, qchi, y2, B, base, out, ippw);
-    else
+    // FP32: grouped kernel; FP64 (register-bound with 2G double sums): one
+    // problem at a time.  Both chunk the batch's active problems.
+    if (shared) {
+      if constexpr (sizeof(T) == 4)
+        k_nufft_interp_group<T><<<dim3(interp_blocks(), interp_chunks()), 256, 0, s>>>(
+            geo, g, gstride, nx, ny, inv_mm, c.st, gate, c.part, qchi, y2, B, base, out, ippw);
+      else
+        k_nufft_interp_shared<T, true><<<dim3(interp_blocks(), interp_chunks()), 256, 0, s>>>(
+            geo, g, gstride, nx, ny, inv_mm, c.st, gate, c.part, qchi, y2, B, base, out, ippw);
+    } else
       k_nufft_interp<T><<<dim3(interp_blocks(), B), 256, 0, s>>>(geo, g, gstride, nx, ny, inv_mm, c.st, gate,
                                                                  c.part, qchi, y2, base, out);
     MF_LAUNCH_CK();
@@ -538,17 +544,17 @@ template <typename T> struct NufftOp : Op {
     const double pts_res = shared ? (double)B * mtot : (double)mtot;  // per-problem residuals
     switch (kernel) {
       case 0:
-        launch_interp(s, g, kGateAll, kQChiX, d_y2.as<cplx<T>>());
+        launch_interp(s, g, kGateTrial, kQChiX, d_y2.as<cplx<T>>());
         return B * G * cs + pts_geo * (8 + 2 * kTaps * ts + 24) + pts_res * cs;
       case 1:
         launch_spread(s, g, kGateGrad);
         return pts_geo * (8 + 2 * kTaps * ts) + pts_res * cs + B * G * cs;
       case 2:
-        launch_rows_fwd(s, c.z, kGateAll, nullptr);
+        launch_rows_fwd(s, c.z, kGateTrial, nullptr);
         return B * N * 8 + N * 8 + B * half_rows * cs;
       case 3:
         k_nufft_cols<T><<<dim3(cdiv(ny + 1, cpc), B), 256, smem_cols, s>>>(g, gstride, nx, ny, fcol.dev, -1, cpc, 1, 0,
-                                                                           c.st, kGateAll);
+                                                                           c.st, kGateTrial);
         MF_LAUNCH_CK();
         return B * (half_rows + G) * cs;
       case 4:
@@ -1259,10 +1265,15 @@ struct Solver {
     build_graph();
   }
 
-  // Autotuner: times each operator kernel alone (profile_kernel, every
-  // problem active) over its candidate shapes, one knob at a time with the
-  // others at their current choice, keeps the fastest and captures the
-  // graph again.  ms_out[k]: best time (ms per launch) for knob k.
+  // Autotuner: times each operator kernel alone (profile_kernel) over its
+  // candidate shapes, one knob at a time with the others at their current
+  // choice, and captures the graph again.  A batched solve runs most of its
+  // iterations with few problems left (the tail of a lambda grid), where
+  // launch shapes that spread one problem over more CTAs win, so every
+  // candidate is timed twice: with the whole batch active (t_all) and with
+  // one problem active (t_one).  The choice minimises
+  // t_all / min t_all + t_one / min t_one.  ms_out[k]: t_all (ms per launch)
+  // of knob k's choice.
   LaunchShapes tune(int reps, double ms_out[4]) {
     LaunchShapes cur = op->shapes();
     // knob -> kernels timed (profile_kernel ids) and candidates
@@ -1277,8 +1288,8 @@ struct Solver {
       ms_out[k] = 0;
       Knob& kb = knobs[k];
       if (cur.*(kb.field) == 0) continue;  // not used by this operator
-      double best = 1e300;
-      int best_v = cur.*(kb.field);
+      std::vector<int> vals;
+      std::vector<double> t_all, t_one;
       for (int v : kb.cand) {
         LaunchShapes tr = cur;
         tr.*(kb.field) = v;
@@ -1288,21 +1299,35 @@ struct Solver {
           continue;  // shape not possible for this problem size
         }
         if (kb.field == &LaunchShapes::spread_cluster && !spread_cluster_fits(v)) continue;
-        double t = 0;
+        double ta = 0, t1 = 0;
         for (int kern : kb.kernels) {
           double ms = 0, by = 0;
           profile_kernel(kern, 1, ms, by);  // warm
           profile_kernel(kern, reps, ms, by);
-          t += ms;
+          ta += ms;
+          profile_kernel(kern, reps, ms, by, 1);
+          t1 += ms;
         }
-        if (t < best) {
-          best = t;
-          best_v = v;
-        }
+        vals.push_back(v);
+        t_all.push_back(ta);
+        t_one.push_back(t1);
       }
-      cur.*(kb.field) = best_v;
+      if (!vals.empty()) {
+        const double ma = *std::min_element(t_all.begin(), t_all.end());
+        const double m1 = *std::min_element(t_one.begin(), t_one.end());
+        size_t best = 0;
+        double best_score = 1e300;
+        for (size_t i = 0; i < vals.size(); ++i) {
+          const double score = t_all[i] / ma + t_one[i] / m1;
+          if (score < best_score) {
+            best_score = score;
+            best = i;
+          }
+        }
+        cur.*(kb.field) = vals[best];
+        ms_out[k] = t_all[best];
+      }
       op->set_shapes(cur);
-      ms_out[k] = best;
     }
     apply_shapes(cur);
     return cur;
@@ -1376,13 +1401,15 @@ struct Solver {
 
   // times one kernel alone: every problem active at the start of an outer
   // iteration, `reps` launches between two events on the solver stream
-  void profile_kernel(int kernel, int reps, double& ms, double& bytes) {
+  // Times one operator kernel alone with the first n_active problems active
+  // (every problem when n_active < 0).
+  void profile_kernel(int kernel, int reps, double& ms, double& bytes, int n_active = -1) {
     std::vector<ProbState> st(ctx.B);
     std::vector<ProbParams> prm(ctx.B);
     MF_CK(cudaMemcpy(prm.data(), ctx.prm, sizeof(ProbParams) * ctx.B, cudaMemcpyDeviceToHost));
     for (int b = 0; b < ctx.B; ++b) {
       memset(&st[b], 0, sizeof(ProbState));
-      st[b].active = 1;
+      st[b].active = (n_active < 0 || b < n_active) ? 1 : 0;
       st[b].need_grad = 1;
       st[b].c = prm[b].cinit > 0 ? prm[b].cinit : 1.0;
     }
