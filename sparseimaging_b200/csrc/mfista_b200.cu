@@ -337,6 +337,7 @@ extern "C" int mfista_plan_run(mfista_plan P) {
   try {
     P->t_start = now_s();
     P->S->steps_host[0] = 0;
+    P->S->steps_host[2] = 0;
     MF_CK(cudaMemcpyAsync(P->S->d_steps.p, P->S->steps_host, sizeof(P->S->steps_host), cudaMemcpyHostToDevice,
                           P->S->stream));
     P->S->enqueue_solve(false);
@@ -353,8 +354,7 @@ extern "C" int mfista_plan_fetch(mfista_plan P, double* xout, struct RESULT* res
     std::vector<FinalOut> o;
     P->S->fetch(xout, o);
     P->comp_time = now_s() - P->t_start;
-    long long steps = P->S->steps_taken();
-    P->launches = (int)(P->S->fixed_launches + steps * P->S->per_step_launches);
+    P->launches = (int)(P->S->fixed_launches + P->S->loop_launches());
     int worst = 0;
     P->statuses.assign(P->B, 0);
     for (int b = 0; b < P->B; ++b) {

@@ -389,4 +389,27 @@ __global__ void k_init_state(ProbState* st, int B, int bad_nonneg_tsv) {
   (void)bad_nonneg_tsv;
 }
 
+
+// Conditional blocks of the device loop: sets the IF handles of the anchor
+// refresh block (has_ref) and of the gradient block for this step -- 1 when
+// some problem needs it -- and counts the kernels that those blocks launch
+// (launched[0]).  One CTA; the blocks' kernels keep their per-problem gates.
+__global__ void k_select_blocks(const ProbState* __restrict__ st, int B, int has_ref,
+                                cudaGraphConditionalHandle h_ref, cudaGraphConditionalHandle h_grad, int n_ref,
+                                int n_grad, unsigned long long* __restrict__ launched) {
+  int g = 0, r = 0;
+  for (int b = threadIdx.x; b < B; b += blockDim.x) {
+    const ProbState& s = st[b];
+    g |= gate_ok(s, kGateGrad) ? 1 : 0;
+    r |= gate_ok(s, kGateRefresh) ? 1 : 0;
+  }
+  g = __syncthreads_or(g);
+  r = __syncthreads_or(r);
+  if (threadIdx.x == 0) {
+    if (has_ref) cudaGraphSetConditional(h_ref, r ? 1u : 0u);
+    cudaGraphSetConditional(h_grad, g ? 1u : 0u);
+    launched[0] += (unsigned long long)((has_ref && r ? n_ref : 0) + (g ? n_grad : 0));
+  }
+}
+
 }  // namespace mf

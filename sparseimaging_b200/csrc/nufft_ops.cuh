@@ -965,7 +965,11 @@ __global__ void __launch_bounds__(256, SharedChunk<T>::kSpreadMinBlocks) k_nufft
   const int tile = blockIdx.x / csize;
   // accumulator slot i holds problem b0 + list[i]: the smallest unrolled
   // width that holds the chunk's active problems
-  if (cnt <= 4)
+  if (cnt == 1)
+    spread_tile<T, PB, 1>(geo, y2, gall, gstride, nx, ny, tile, b0, cnt, sm, s_acc, cluster, rank, csize);
+  else if (cnt == 2)
+    spread_tile<T, PB, 2>(geo, y2, gall, gstride, nx, ny, tile, b0, cnt, sm, s_acc, cluster, rank, csize);
+  else if (cnt <= 4)
     spread_tile<T, PB, 4>(geo, y2, gall, gstride, nx, ny, tile, b0, cnt, sm, s_acc, cluster, rank, csize);
   else if (PB > 8 && cnt <= 8)
     spread_tile<T, PB, (PB > 8 ? 8 : PB)>(geo, y2, gall, gstride, nx, ny, tile, b0, cnt, sm, s_acc, cluster, rank,

@@ -999,7 +999,7 @@ struct Solver {
   DevMem d_x, d_z, d_xnew, d_dfdx, d_xa, d_prm, d_st, d_part, d_out, d_box, d_fgp, d_steps, d_ticket;
   unsigned long long step_budget = 0;
   ImgDims dm{};
-  cudaStream_t stream = nullptr, cap_stream = nullptr;
+  cudaStream_t stream = nullptr, cap_stream = nullptr, cap_block = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t body_graph = nullptr;  // host-loop fallback
@@ -1014,6 +1014,10 @@ struct Solver {
   long fgp_scratch_stride = 0;
   int per_step_launches = 0;
   int fixed_launches = 0;
+  int ref_block_launches = 0, grad_block_launches = 0, rest_launches = 0;
+  // device loop with conditional IF blocks: the refresh and gradient blocks
+  // run only in steps where some problem needs them (k_select_blocks)
+  bool cond_blocks = false;
   const float* box_ptr = nullptr;
 
   Solver() {}
@@ -1025,6 +1029,7 @@ struct Solver {
     if (h_any) cudaFreeHost(h_any);
     if (stream) cudaStreamDestroy(stream);
     if (cap_stream) cudaStreamDestroy(cap_stream);
+    if (cap_block) cudaStreamDestroy(cap_block);
   }
 
   void init_common(int B, int N, int NX, int NY, int form_, int fgp_iter_, const float* box) {
@@ -1037,6 +1042,7 @@ struct Solver {
     fgp_iter = fgp_iter_;
     MF_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     MF_CK(cudaStreamCreateWithFlags(&cap_stream, cudaStreamNonBlocking));
+    MF_CK(cudaStreamCreateWithFlags(&cap_block, cudaStreamNonBlocking));
     d_x.alloc(sizeof(double) * (size_t)B * N);
     d_z.alloc(sizeof(double) * (size_t)B * N);
     d_xnew.alloc(sizeof(double) * (size_t)B * N);
@@ -1044,7 +1050,7 @@ struct Solver {
     d_prm.alloc(sizeof(ProbParams) * B);
     d_st.alloc(sizeof(ProbState) * B);
     d_out.alloc(sizeof(FinalOut) * B);
-    d_steps.alloc(2 * sizeof(unsigned long long));
+    d_steps.alloc(3 * sizeof(unsigned long long));
     d_ticket.alloc(sizeof(unsigned int));
     MF_CK(cudaMemset(d_ticket.p, 0, sizeof(unsigned int)));
     ctx.x = d_x.as<double>();
@@ -1081,9 +1087,12 @@ struct Solver {
     refresh_every = op->corrected() ? op->refresh_period() : 0;
     if (const char* re = getenv("MFISTA_REFRESH_EVERY"))  // anchor refresh period (tuning)
       if (op->corrected() && atoi(re) > 0) refresh_every = atoi(re);
-    per_step_launches = op->launches_forward() * (op->models_z() ? 1 : 2) + op->launches_adjoint() + 3 +
-                        (form == kFormTV ? 1 : 0) + (op->corrected() ? 1 + op->launches_refresh() : 0) +
-                        (op->models_z() ? 2 : 0);
+    // kernels per loop step: the anchor refresh block, the gradient block
+    // and the rest (trial point, its forward pass, control, momentum)
+    ref_block_launches = op->corrected() ? 1 + op->launches_refresh() : 0;
+    grad_block_launches = (op->models_z() ? 1 : op->launches_forward()) + op->launches_adjoint();
+    rest_launches = op->launches_forward() + 3 + (form == kFormTV ? 1 : 0) + (op->models_z() ? 1 : 0);
+    per_step_launches = ref_block_launches + grad_block_launches + rest_launches;
     fixed_launches = 2 * (op->launches_forward() + 2) + 1;
     const char* hl = getenv("MFISTA_HOST_LOOP");
     host_loop = hl && hl[0] == '1';
@@ -1219,19 +1228,62 @@ struct Solver {
     MF_LAUNCH_CK();
   }
 
-  void enqueue_body(cudaStream_t s, cudaGraphConditionalHandle h, int set_handle) {
+  // Adds an IF node (condition hc) at the capture position of s and starts
+  // capturing its body on cap_block; returns the stream to enqueue it on.
+  cudaStream_t begin_if(cudaStream_t s, cudaGraphConditionalHandle hc) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    MF_CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = hc;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    MF_CK(cudaGraphAddNode(&node, g, deps, nd, &cp));
+    MF_CK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    MF_CK(cudaStreamBeginCaptureToGraph(cap_block, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal));
+    return cap_block;
+  }
+  void end_if() {
+    cudaGraph_t out;
+    MF_CK(cudaStreamEndCapture(cap_block, &out));
+  }
+
+  // One loop step.  cond: inside the device loop's WHILE body, with the
+  // refresh and gradient blocks under IF nodes set by k_select_blocks.
+  void enqueue_body(cudaStream_t s, cudaGraphConditionalHandle h, int set_handle, bool cond = false) {
     dim3 ig(img_blocks(), ctx.B);
-    if (op->corrected()) {  // new FP64 anchor x_a = x every refresh_every outer iterations
-      k_copy_gated<<<ig, 256, 0, s>>>(ctx.xa, ctx.x, dm, ctx.st, kGateRefresh);
+    cudaGraphConditionalHandle h_ref = 0, h_grad = 0;
+    if (cond) {
+      cudaStreamCaptureStatus cs;
+      cudaGraph_t g = nullptr;
+      MF_CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, nullptr, nullptr));
+      if (op->corrected()) MF_CK(cudaGraphConditionalHandleCreate(&h_ref, g, 0, 0));
+      MF_CK(cudaGraphConditionalHandleCreate(&h_grad, g, 0, 0));
+      k_select_blocks<<<1, 256, 0, s>>>(ctx.st, ctx.B, op->corrected() ? 1 : 0, h_ref, h_grad, ref_block_launches,
+                                        grad_block_launches, d_steps.as<unsigned long long>() + 2);
       MF_LAUNCH_CK();
-      op->refresh_anchor(s, kGateRefresh);
     }
-    // gradient at z (only problems that start a new outer iteration)
-    if (op->models_z()) op->forward_z(s, kGateGrad, kQChiZ);
-    else op->forward(s, ctx.z, kGateGrad, kQChiZ, true);
-    // the adjoint folds in the TSV gradient of z; TSV(z) itself is reduced by
-    // k_update_tsv with the same tree as TSV(xnew)
-    op->adjoint(s, form == kFormTSV ? ctx.z : nullptr, -1);
+    if (op->corrected()) {  // new FP64 anchor x_a = x every refresh_every outer iterations
+      cudaStream_t bs = cond ? begin_if(s, h_ref) : s;
+      k_copy_gated<<<ig, 256, 0, bs>>>(ctx.xa, ctx.x, dm, ctx.st, kGateRefresh);
+      MF_LAUNCH_CK();
+      op->refresh_anchor(bs, kGateRefresh);
+      if (cond) end_if();
+    }
+    {
+      cudaStream_t bs = cond ? begin_if(s, h_grad) : s;
+      // gradient at z (only problems that start a new outer iteration)
+      if (op->models_z()) op->forward_z(bs, kGateGrad, kQChiZ);
+      else op->forward(bs, ctx.z, kGateGrad, kQChiZ, true);
+      // the adjoint folds in the TSV gradient of z; TSV(z) itself is reduced by
+      // k_update_tsv with the same tree as TSV(xnew)
+      op->adjoint(bs, form == kFormTSV ? ctx.z : nullptr, -1);
+      if (cond) end_if();
+    }
     // trial point
     if (form == kFormTSV) {
       k_update_tsv<<<ig, 256, 0, s>>>(ctx.z, ctx.dfdx, ctx.xnew, dm, ctx.prm, ctx.st, box_ptr, ctx.part);
@@ -1341,6 +1393,7 @@ struct Solver {
   }
 
   void build_graph() {
+    cond_blocks = false;
     if (!host_loop) {
       cudaError_t e = try_build_conditional();
       if (e == cudaSuccess) return;
@@ -1371,15 +1424,19 @@ struct Solver {
                                            cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
       return e;
     try {
-      enqueue_body(cap_stream, h, 1);
+      enqueue_body(cap_stream, h, 1, true);
     } catch (...) {
       cudaGraph_t tmp;
+      cudaStreamEndCapture(cap_block, &tmp);
       cudaStreamEndCapture(cap_stream, &tmp);
-      throw;
+      cudaGetLastError();
+      return cudaErrorNotSupported;  // falls back to the host loop
     }
     cudaGraph_t out;
     if ((e = cudaStreamEndCapture(cap_stream, &out)) != cudaSuccess) return e;
-    return cudaGraphInstantiate(&exec, graph, 0);
+    if ((e = cudaGraphInstantiate(&exec, graph, 0)) != cudaSuccess) return e;
+    cond_blocks = true;
+    return cudaSuccess;
   }
 
   // params: per problem; x0: [B*N] host (null = zeros); skip_loop: start
@@ -1395,9 +1452,12 @@ struct Solver {
     for (const ProbParams& p : prm) mx = std::max<long long>(mx, p.maxiter);
     steps_host[0] = 0;
     steps_host[1] = (unsigned long long)(mx * 64 + 4096);
+    steps_host[2] = 0;
     MF_CK(cudaMemcpyAsync(d_steps.p, steps_host, sizeof(steps_host), cudaMemcpyHostToDevice, stream));
   }
-  unsigned long long steps_host[2] = {0, 0};
+  // [0] loop steps taken, [1] step budget, [2] kernels launched by the
+  // conditional blocks
+  unsigned long long steps_host[3] = {0, 0, 0};
 
   // times one kernel alone: every problem active at the start of an outer
   // iteration, `reps` launches between two events on the solver stream
@@ -1444,9 +1504,16 @@ struct Solver {
   }
 
   long long steps_taken() {
-    unsigned long long h[2];
+    unsigned long long h[3];
     MF_CK(cudaMemcpy(h, d_steps.p, sizeof(h), cudaMemcpyDeviceToHost));
     return (long long)h[0];
+  }
+  // kernels launched by the last solve's loop
+  long long loop_launches() {
+    unsigned long long h[3];
+    MF_CK(cudaMemcpy(h, d_steps.p, sizeof(h), cudaMemcpyDeviceToHost));
+    if (!cond_blocks) return (long long)h[0] * per_step_launches;
+    return (long long)h[0] * (rest_launches + 1) + (long long)h[2];
   }
 
   void enqueue_solve(bool skip_loop) {

@@ -126,3 +126,33 @@ def test_fp32_defect_corrected_reaches_fp64_objective(gpulib, c0):
         assert r["finalcost"] <= t, (b, r["finalcost"], t)
         assert r["ITER"] < 4000
         assert rel(X32[b], X64[b]) < 2e-2
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_device_loop_matches_host_loop(gpulib, c0, precision, monkeypatch):
+    """The device loop (CUDA graph WHILE node whose anchor-refresh and
+    gradient blocks sit under IF nodes, skipped in steps that need neither)
+    gives the host loop's bits (every kernel launched each step, gated per
+    problem).  With anchor refreshes every 32 iterations (FP32 form) it
+    launches fewer kernels; FP64 has no refresh block, and its gradient
+    block is skipped only in backtracking retries."""
+    prec = gpulib.FP32 if precision == "fp32" else gpulib.FP64
+    probs = _problems(c0, [0.4, 1.0, 3.0], 120)
+    args = (c0["u"], c0["v"], c0["vis_r"], c0["vis_i"], c0["vis_std"], 64, 64, len(probs))
+    out = {}
+    for mode in ("device", "host"):
+        if mode == "host":
+            monkeypatch.setenv("MFISTA_HOST_LOOP", "1")
+        plan = gpulib.Plan(*args, precision=prec)
+        plan.set_problems(probs, 1e-5)
+        plan.run()
+        X, R = plan.fetch()
+        out[mode] = (X, R, plan.kernel_launches, plan.device_loop)
+        plan.close()
+    (Xd, Rd, Ld, dd), (Xh, Rh, Lh, dh) = out["device"], out["host"]
+    assert dd and not dh
+    assert np.array_equal(Xd, Xh)
+    assert [r["ITER"] for r in Rd] == [r["ITER"] for r in Rh]
+    assert [r["finalcost"] for r in Rd] == [r["finalcost"] for r in Rh]
+    if precision == "fp32":
+        assert Ld < Lh
