@@ -265,6 +265,20 @@ int mfista_dft_apply(const double *A, int M, int N, const double *X, int B, int 
 int mfista_dft_profile(const double *A, int M, int N, int B, int precision, int kernel, int reps,
                        double *ms_per_launch, double *bytes_per_launch);
 
+/* Approximate leave-one-out error (LOOE) of B solutions X [B][N] of the DFT
+ * problem y [M] = A [M x N, column-major] x: the reference's
+ * compute_LOOE_L1 / compute_LOOE_L1_TSV (c/looe_lib.c:190-226, :275-309;
+ * its call in c/mfista_dft_lib.c:506-529 is commented out and the reference
+ * does not build the file) on the GPU in FP64.  From the active set S of x:
+ * H = A_S^T A_S (+ lambda_tsv[b] times the TSV Hessian diagonal 8/6/4 of
+ * the NX grid), d_i = (A_S H^-1 A_S^T)_ii, t_i = (y - A x)_i / (1 - d_i);
+ * looe_m[b] = mean t_i^2/2 and looe_std[b] their spread as the reference
+ * forms it.  hessian_positive[b] = 0 when H is not positive definite (then
+ * looe_m = looe_std = 0, the reference's -1 return).  lambda_tsv may be
+ * NULL (L1 form for every solution).  Needs M >= 2. */
+int mfista_dft_looe(const double *y, const double *A, int M, int N, int NX, const double *X, int B,
+                    const double *lambda_tsv, double *looe_m, double *looe_std, int *hessian_positive);
+
 /* FGP TV proximal map alone (FGP_L1_box / FGP_nonneg_box,
  * c/mfista_TV_lib.c:189-384) on an NX x NY view: x_out = prox(b). */
 int mfista_fgp_prox(const double *b, int NX, int NY, double lambda_l1, double lambda_tv,

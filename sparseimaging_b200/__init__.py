@@ -131,6 +131,8 @@ def lib():
         L.mfista_dft_apply.argtypes = [_dp, C.c_int, C.c_int, _dp, C.c_int, C.c_int, C.c_int, _dp]
         L.mfista_dft_profile.restype = C.c_int
         L.mfista_dft_profile.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]
+        L.mfista_dft_looe.restype = C.c_int
+        L.mfista_dft_looe.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp, _dp, _ip]
         L.mfista_plan_destroy.restype = None
         L.mfista_plan_destroy.argtypes = [C.c_void_p]
         L.mfista_nufft_forward.restype = C.c_int
@@ -357,6 +359,24 @@ def dft_profile(A, B, kernel, precision=None, reps=20):
     _check(lib().mfista_dft_profile(Af.ctypes.data_as(_dp), m, n, B, precision, kernel, reps, C.byref(ms),
                                     C.byref(by)))
     return ms.value, by.value
+
+
+def dft_looe(y, A, X, nx, lambda_tsv=None):
+    """Approximate leave-one-out error of DFT solutions (the reference's
+    c/looe_lib.c) on the GPU: A is (M, N), X the solutions [B][N] (e.g. a
+    lambda grid's from dft_batch), lambda_tsv None (L1 form) or per
+    solution.  Returns (looe_m [B], looe_std [B], hessian_positive [B])."""
+    A = np.asarray(A, np.float64)
+    m, n = A.shape
+    Af = np.asfortranarray(A)
+    X = np.ascontiguousarray(np.atleast_2d(X), np.float64)
+    B = X.shape[0]
+    lt = None if lambda_tsv is None else _d(np.broadcast_to(np.asarray(lambda_tsv, np.float64), (B,)))
+    om, osd = np.zeros(B), np.zeros(B)
+    pos = np.zeros(B, np.int32)
+    _check(lib().mfista_dft_looe(_p(_d(y)), Af.ctypes.data_as(_dp), m, n, nx, _p(X), B, _p(lt), _p(om), _p(osd),
+                                 pos.ctypes.data_as(_ip)))
+    return om, osd, pos.astype(bool)
 
 
 class Plan:

@@ -7,6 +7,7 @@
 #include <time.h>
 
 #include "solver.cuh"
+#include "looe.cuh"
 
 using namespace mf;
 
@@ -729,6 +730,28 @@ extern "C" int mfista_fgp_prox(const double* b, int NX, int NY, double lambda_l1
     S.launch_fgp(S.stream);
     MF_CK(cudaMemcpyAsync(x_out, S.ctx.xnew, sizeof(double) * n, cudaMemcpyDeviceToHost, S.stream));
     MF_CK(cudaStreamSynchronize(S.stream));
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
+// leave-one-out error of DFT solutions (c/looe_lib.c, see looe.cuh)
+extern "C" int mfista_dft_looe(const double* y, const double* A, int M, int N, int NX, const double* X, int B,
+                               const double* lambda_tsv, double* looe_m, double* looe_std, int* hessian_positive) {
+  set_ok();
+  try {
+    if (M < 2 || N < 1 || NX < 1 || B < 1) throw Error(MFISTA_ERR_ARG, "mfista_dft_looe: needs M >= 2, N, NX, B >= 1");
+    if (!y || !A || !X || !looe_m || !looe_std || !hessian_positive)
+      throw Error(MFISTA_ERR_ARG, "mfista_dft_looe: null pointer");
+    looe::Looe L(y, A, M, N, NX);
+    for (int b = 0; b < B; ++b) {
+      double out[3];
+      L.one(X + (size_t)b * N, lambda_tsv ? lambda_tsv[b] : 0.0, out);
+      looe_m[b] = out[0];
+      looe_std[b] = out[1];
+      hessian_positive[b] = out[2] > 0.5 ? 1 : 0;
+    }
     return MFISTA_OK;
   } catch (const Error& e) {
     return fail(e.status, e.what(), false);
