@@ -104,14 +104,43 @@ def dft_lambda_grid(si):
         return {"unavailable": "F* fixture does not match the DFT workload"}
     targets = np.array(fx["fstar"]) * (1 + REL_OBJ)
     out = {"workload": f"DFT {p.nx}x{p.nx}, A {p.A.shape[0]}x{p.A.shape[1]}, 64-problem lambda grid"}
+    X64 = None
     for name, prec in (("fp64", si.FP64), ("bf16x6", si.BF16X6), ("bf16x3", si.BF16X3)):
-        _, R = si.dft_batch(p.y, p.A, p.nx, p.nx, D.problems(grid, lip, 30000, targets), 0.0, precision=prec)
+        X, R = si.dft_batch(p.y, p.A, p.nx, p.nx, D.problems(grid, lip, 30000, targets), 0.0, precision=prec)
+        if X64 is None:
+            X64 = X
         secs = R[0]["comp_time"]
         out[name] = {"solves_per_s": round(len(grid) / secs, 3), "solve_s": round(secs, 4),
                      "reached_1e-6": int(sum(r["finalcost"] <= t for r, t in zip(R, targets))),
                      "max_iters": int(max(r["ITER"] for r in R))}
     out["speedup_bf16x6_vs_fp64"] = round(out["fp64"]["solve_s"] / out["bf16x6"]["solve_s"], 2)
+    out["looe"] = dft_looe_side(si, p, X64, [float(lt) for _, lt in grid])
     return out
+
+
+def dft_looe_side(si, p, X, lts):
+    """Leave-one-out error (the reference's c/looe_lib.c) of the 64 FP64
+    lambda-grid solutions: one mfista_dft_looe call (A upload included)
+    against the oracle's numpy/LAPACK restatement on the host for every 4th
+    solution (scaled by 4)."""
+    from oracle import looe_oracle as O
+    ns = [int(np.count_nonzero(x)) for x in X]
+    t = time.perf_counter()
+    m, sd, pos = si.dft_looe(p.y, p.A, X, p.nx, lambda_tsv=lts)
+    gpu_s = time.perf_counter() - t
+    sample = list(range(0, len(X), 4))
+    t = time.perf_counter()
+    worst = 0.0
+    for b in sample:
+        st, wm, _ = O.looe(p.y, p.A, X[b], p.nx, lts[b])
+        if st and pos[b]:
+            worst = max(worst, abs(m[b] - wm) / abs(wm))
+    cpu_s = (time.perf_counter() - t) * len(X) / len(sample)
+    return {"solutions": len(X), "active_pixels": {"min": min(ns), "mean": int(np.mean(ns)), "max": max(ns)},
+            "gpu_s": round(gpu_s, 4), "hessian_positive": int(pos.sum()),
+            "cpu_baseline": {"seconds": round(cpu_s, 3), "kind": "port", "cores": os.cpu_count(),
+                             "sample": f"numpy/LAPACK restatement on {len(sample)} of {len(X)} solutions, x{len(X) // len(sample)}"},
+            "speedup_vs_cpu": round(cpu_s / gpu_s, 1), "max_rel_diff_looe_m": worst}
 
 
 def movie_batch(si):
