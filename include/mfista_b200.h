@@ -157,6 +157,27 @@ int mfista_nufft_batch(const double *u_dx, const double *v_dy, const double *vis
                        int fgp_iter, const double *xinit, double *xout,
                        struct RESULT *results);
 
+/* Movie: n_frames images of one source, solved as ONE problem
+ *   min sum_b [ chi2_b(x_b)/2 + lambda_l1 |x_b|_1 + lambda_tsv TSV(x_b) ]
+ *       + lambda_t sum_b |x_b - x_{b+1}|^2 / (t_{b+1} - t_b)
+ * by MFISTA with one joint step size, momentum, backtracking test and
+ * stopping rule (the reference's matlab/MFISTA_movie_eht.m:93-194, with
+ * d_X / dt_X of matlab/lib; its NUFFT is FINUFFT, here every frame uses
+ * this library's NUFFT, i.e. the C reference's gridding).  Frame b uses
+ * points [pt_off[b], pt_off[b+1]).  t_list: n_frames increasing frame times,
+ * or NULL for 1, 2, ...  eps is used as given (the matlab code does not
+ * scale it).  xinit: one Nx*Ny image replicated to every frame, or NULL.
+ * xout: [n_frames*Nx*Ny]; results: [n_frames] per-frame terms (finalcost
+ * without the temporal term; ITER and Lip_const are the joint ones);
+ * temporal_cost: lambda_t times the temporal sum at xout (may be NULL).
+ * FP64, TSV form (the matlab code has no TV form), no box constraint.
+ * No counterpart in the reference's C library. */
+int mfista_nufft_movie(const double *u_dx, const double *v_dy, const double *vis_r, const double *vis_i,
+                       const double *vis_std, const int *pt_off, int n_frames, int Nx, int Ny,
+                       const double *t_list, double lambda_l1, double lambda_tsv, double lambda_t,
+                       double cinit, int maxiter, double eps, int nonneg_flag, const double *xinit,
+                       double *xout, struct RESULT *results, double *temporal_cost);
+
 /* Batched DFT solve (B problems sharing the column-major M x N matrix A and
  * the data y, e.g. a lambda grid): A z and A^T r run as GEMMs over the
  * batch.  eps is used raw, as mfista_imaging_core_dft does.  precision: 64. */

@@ -131,6 +131,10 @@ def lib():
         L.mfista_dft_apply.argtypes = [_dp, C.c_int, C.c_int, _dp, C.c_int, C.c_int, C.c_int, _dp]
         L.mfista_dft_profile.restype = C.c_int
         L.mfista_dft_profile.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]
+        L.mfista_nufft_movie.restype = C.c_int
+        L.mfista_nufft_movie.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, C.c_int, C.c_int, C.c_int, _dp, C.c_double,
+                                         C.c_double, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int, _dp,
+                                         _dp, C.POINTER(RESULT), _dp]
         L.mfista_dft_looe.restype = C.c_int
         L.mfista_dft_looe.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp, _dp, _ip]
         L.mfista_plan_destroy.restype = None
@@ -359,6 +363,26 @@ def dft_profile(A, B, kernel, precision=None, reps=20):
     _check(lib().mfista_dft_profile(Af.ctypes.data_as(_dp), m, n, B, precision, kernel, reps, C.byref(ms),
                                     C.byref(by)))
     return ms.value, by.value
+
+
+def nufft_movie(u_dx, v_dy, vis_r, vis_i, vis_std, pt_off, nx, ny, lambda_l1, lambda_tsv, lambda_t, cinit,
+                maxiter, eps, nonneg_flag=1, t_list=None, xinit=None):
+    """Movie of len(pt_off) - 1 frames solved as one problem with the
+    temporal term lambda_t sum_b |x_b - x_{b+1}|^2 / (t_{b+1} - t_b)
+    (mfista_nufft_movie).  Returns (X [T][nx*ny], per-frame RESULT dicts,
+    temporal cost at X)."""
+    u, v, vr, vi, vs = (_d(a) for a in (u_dx, v_dy, vis_r, vis_i, vis_std))
+    off = np.ascontiguousarray(pt_off, np.int32)
+    T = off.size - 1
+    xo = np.zeros(T * nx * ny)
+    res = (RESULT * T)()
+    tc = C.c_double(0)
+    tl = None if t_list is None else _d(t_list)
+    xi = None if xinit is None else _d(xinit)
+    _check(lib().mfista_nufft_movie(_p(u), _p(v), _p(vr), _p(vi), _p(vs), off.ctypes.data_as(_ip), T, nx, ny,
+                                    _p(tl), lambda_l1, lambda_tsv, lambda_t, cinit, maxiter, eps, nonneg_flag,
+                                    _p(xi), _p(xo), res, C.byref(tc)))
+    return xo.reshape(T, nx * ny), [r.as_dict() for r in res], tc.value
 
 
 def dft_looe(y, A, X, nx, lambda_tsv=None):

@@ -93,6 +93,8 @@ enum Quantity {
   kQL1,         // |v|_1
   kQReg,        // TSV(v) or TV(v)
   kQNact,       // number of nonzero pixels (final summary)
+  kQDtZ,        // movie: temporal term sum_i (z_b - z_{b+1})^2 / dt_b at z
+  kQDtX,        // movie: the same at the trial point / x
   kNumQ
 };
 

@@ -757,3 +757,61 @@ extern "C" int mfista_dft_looe(const double* y, const double* A, int M, int N, i
     return fail(e.status, e.what(), false);
   }
 }
+
+// movie: frames coupled by a temporal term (matlab/MFISTA_movie_eht.m)
+extern "C" int mfista_nufft_movie(const double* u_dx, const double* v_dy, const double* vis_r, const double* vis_i,
+                                  const double* vis_std, const int* pt_off, int n_frames, int Nx, int Ny,
+                                  const double* t_list, double lambda_l1, double lambda_tsv, double lambda_t,
+                                  double cinit, int maxiter, double eps, int nonneg_flag, const double* xinit,
+                                  double* xout, struct RESULT* results, double* temporal_cost) {
+  set_ok();
+  try {
+    if (n_frames < 1 || Nx < 1 || Ny < 1) throw Error(MFISTA_ERR_ARG, "mfista_nufft_movie: bad sizes");
+    if (!u_dx || !v_dy || !vis_r || !vis_i || !vis_std || !pt_off || !xout)
+      throw Error(MFISTA_ERR_ARG, "mfista_nufft_movie: null pointer");
+    if (maxiter < 0) throw Error(MFISTA_ERR_ARG, "maxiter must be >= 0");
+    if (nonneg_flag != 0 && nonneg_flag != 1) throw Error(MFISTA_ERR_ARG, "nonneg_flag must be 0 or 1");
+    if (lambda_t < 0 || lambda_tsv < 0) throw Error(MFISTA_ERR_ARG, "lambda_t and lambda_tsv must be >= 0");
+    std::vector<double> wt(std::max(n_frames - 1, 0));
+    for (int b = 0; b + 1 < n_frames; ++b) {
+      const double dt = t_list ? t_list[b + 1] - t_list[b] : 1.0;
+      if (!(dt > 0)) throw Error(MFISTA_ERR_ARG, "t_list must increase strictly");
+      wt[b] = 1.0 / dt;
+    }
+    const int N = Nx * Ny;
+    Solver S;
+    S.precision = MFISTA_FP64;
+    S.init_common(n_frames, N, Nx, Ny, kFormTSV, 100, nullptr);
+    NufftInput in{u_dx, v_dy, vis_r, vis_i, vis_std, pt_off, 0, 0, Nx, Ny};
+    S.op.reset(new NufftOp<double>(S.ctx, in));
+    S.set_movie(wt, lambda_t);
+    S.finish_setup();
+    std::vector<ProbParams> prm(n_frames);
+    for (int b = 0; b < n_frames; ++b)
+      prm[b] = ProbParams{lambda_l1, 0.0, lambda_tsv, cinit, eps, maxiter, nonneg_flag, 0, 0, 0.0};
+    std::vector<double> x0;
+    if (xinit) {
+      x0.resize((size_t)n_frames * N);
+      for (int b = 0; b < n_frames; ++b) std::copy(xinit, xinit + N, x0.begin() + (size_t)b * N);
+    }
+    double t0 = now_s();
+    S.upload_problems(prm, xinit ? x0.data() : nullptr);
+    S.enqueue_solve(false);
+    std::vector<FinalOut> o;
+    S.fetch(xout, o);
+    const double ct = now_s() - t0;
+    double dx = 0.0;
+    for (int b = 0; b < n_frames; ++b) dx += o[b].dt_pair;
+    if (temporal_cost) *temporal_cost = lambda_t * dx;
+    if (results)
+      for (int b = 0; b < n_frames; ++b) {
+        const int m = pt_off[b + 1] - pt_off[b];
+        fill_result(&results[b], o[b], m / 2, (double)m, Nx, Ny, N, lambda_l1, 0.0, lambda_tsv, maxiter, nonneg_flag, ct,
+                    false, cinit);
+      }
+    if (o[0].status) return fail(o[0].status, "the movie stopped early (status " + std::to_string(o[0].status) + ")", false);
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}

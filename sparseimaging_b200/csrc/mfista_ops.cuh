@@ -195,6 +195,53 @@ __global__ void k_copy_gated(double* __restrict__ dst, const double* __restrict_
 }
 
 // ---------------------------------------------------------------------------
+// movie: frames coupled by lam_t sum_b sum_i (x_b,i - x_{b+1},i)^2 wt_b,
+// wt_b = 1 / (t_{b+1} - t_b)  (matlab/lib/d_X.m, matlab/lib/dt_X.m)
+// ---------------------------------------------------------------------------
+// gradient step: dfdx_b -= lam_t dtX(z)_b with
+//   dtX_b = 2 (z_b - z_{b+1}) wt_b - 2 (z_{b-1} - z_b) wt_{b-1}
+// (missing neighbours drop out), and the partial sums of the pair term
+// (z_b - z_{b+1})^2 wt_b into kQDtZ
+__global__ void k_movie_tgrad(const double* __restrict__ zall, double* __restrict__ dall, ImgDims dm,
+                              const double* __restrict__ wt, double lam_t, const ProbState* __restrict__ st,
+                              Partials part) {
+  __shared__ double sh[32];
+  const int b = blockIdx.y, B = gridDim.y;
+  if (!gate_ok(st[b], kGateGrad)) return;
+  double acc[1] = {0.0};
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < dm.N) {
+    const double zb = zall[(size_t)b * dm.xstride + f];
+    double g = 0.0;
+    if (b + 1 < B) {
+      const double d = zb - zall[(size_t)(b + 1) * dm.xstride + f];
+      g += 2 * d * wt[b];
+      acc[0] = d * d * wt[b];
+    }
+    if (b > 0) g -= 2 * (zall[(size_t)(b - 1) * dm.xstride + f] - zb) * wt[b - 1];
+    dall[(size_t)b * dm.xstride + f] -= lam_t * g;
+  }
+  block_sum<1>(acc, sh);
+  if (threadIdx.x == 0) part.at(kQDtZ, b)[blockIdx.x] = acc[0];
+}
+
+// partial sums of the pair term (v_b - v_{b+1})^2 wt_b into kQDtX
+__global__ void k_movie_dx(const double* __restrict__ vall, ImgDims dm, const double* __restrict__ wt,
+                           const ProbState* __restrict__ st, int gate, Partials part) {
+  __shared__ double sh[32];
+  const int b = blockIdx.y, B = gridDim.y;
+  if (!gate_ok(st[b], gate)) return;
+  double acc[1] = {0.0};
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < dm.N && b + 1 < B) {
+    const double d = vall[(size_t)b * dm.xstride + f] - vall[(size_t)(b + 1) * dm.xstride + f];
+    acc[0] = d * d * wt[b];
+  }
+  block_sum<1>(acc, sh);
+  if (threadIdx.x == 0) part.at(kQDtX, b)[blockIdx.x] = acc[0];
+}
+
+// ---------------------------------------------------------------------------
 // control
 // ---------------------------------------------------------------------------
 enum CtrlMode { kCtrlInit = 0, kCtrlStep = 1, kCtrlFinal = 2 };
@@ -214,6 +261,13 @@ struct CtrlCfg {
   // the corrected low-precision forms, whose F and Q come from differently
   // rounded operator paths
   double bt_slack;
+  // movie mode: the B problems are the frames of ONE problem with the
+  // temporal term lam_t sum_b |x_b - x_{b+1}|^2 / dt_b; one joint c, mu,
+  // cost and backtracking decision for all frames.  jq: [B][kNumQ] scratch
+  // for the frames' reduced quantities.
+  int joint;
+  double lam_t;
+  double* jq;
 };
 
 // status codes written to ProbState.status (values of enum mfista_status)
@@ -224,6 +278,7 @@ struct FinalOut {       // one per problem, read back by the host
   double sq_error, l1cost, regcost, finalcost;
   double n_active;
   double lip;
+  double dt_pair;       // movie: sum_i (x_b - x_{b+1})^2 / dt_b (0 for the last frame)
   int iters;
   int status;
 };
@@ -232,6 +287,113 @@ __device__ __forceinline__ double warp_partial_sum(const double* p, int n, int l
   double s = 0.0;
   for (int i = lane; i < n; i += 32) s += p[i];
   return warp_sum(s);
+}
+
+// Movie mode, init and step (matlab/MFISTA_movie_eht.m:93-194): every CTA
+// has reduced its frame's quantities into red[]; they go to cfg.jq, and the
+// last CTA to arrive sums them over the frames in order and runs the scalar
+// logic once for the whole movie:
+//   F = sum_b (chi2_b / 2 + lambda_tsv TSV_b) + lam_t dX,  Q likewise at z,
+// one backtracking test, one c and mu, one cost ring and stopping rule, and
+// the same state written to every frame.  The matlab code has no "x
+// becomes a 0 vector" stop; its backtracking also ends once c > 1e200.
+__device__ void control_joint(const ProbParams* __restrict__ prm, ProbState* __restrict__ st, const CtrlCfg& cfg,
+                              const double* red, cudaGraphConditionalHandle handle, int set_handle,
+                              int* __restrict__ any_active, unsigned int* __restrict__ ticket) {
+  const int b = blockIdx.x;
+  if (threadIdx.x != 0) return;
+  for (int q = 0; q < kNumQ; ++q) cfg.jq[(size_t)b * kNumQ + q] = red[q];
+  __threadfence();
+  const unsigned int t = atomicAdd(ticket, 1u);
+  if (t != gridDim.x - 1) return;
+  __threadfence();
+  double tot[kNumQ];
+  for (int q = 0; q < kNumQ; ++q) tot[q] = 0.0;
+  for (int k = 0; k < (int)gridDim.x; ++k)
+    for (int q = 0; q < kNumQ; ++q) tot[q] += ((volatile double*)cfg.jq)[(size_t)k * kNumQ + q];
+  // the frames' states are identical and no CTA of this launch writes them
+  ProbState s = st[0];
+  const ProbParams p = prm[0];
+  const bool tsv_on = p.lambda_tsv > 0;
+  if (cfg.mode == kCtrlInit) {
+    s.cost_now = cfg.fscale * tot[kQChiX] + p.lambda_l1 * tot[kQL1] + (tsv_on ? p.lambda_tsv * tot[kQReg] : 0.0);
+    s.l1x = tot[kQL1];
+    s.c = p.cinit;
+    s.mu = 1.0;
+    s.iter = 0;
+    s.trial = 0;
+    s.iters_out = 0;
+    s.accepted = 0;
+    s.take_x = 0;
+    s.active = (p.maxiter > 0 && s.status == 0) ? 1 : 0;
+    s.need_grad = s.active;
+    s.refresh = 0;
+  } else if (!s.active) {
+    s.accepted = 0;
+  } else {
+    const bool capped = cfg.steps && (cfg.steps[0] + 1ull >= cfg.steps[1]);
+    if (s.need_grad) {
+      s.cost[s.iter % kCostRing] = s.cost_now;
+      s.qcore = cfg.fscale * tot[kQChiZ] + (tsv_on ? p.lambda_tsv * tot[kQTsvZ] : 0.0) + cfg.lam_t * tot[kQDtZ];
+      s.trial = 0;
+      s.need_grad = 0;
+      s.refresh = 0;
+    }
+    s.accepted = 0;
+    double fval = cfg.fscale * tot[kQChiX] + (tsv_on ? p.lambda_tsv * tot[kQReg] : 0.0) + cfg.lam_t * tot[kQDtX];
+    const double qval = (-tot[kQDq1] + s.c * tot[kQDq2] / 2) + s.qcore;
+    if (isnan(fval) || isnan(qval) || capped) {
+      s.status = capped ? kStatusStepCap : kStatusNonFinite;
+      s.active = 0;
+      s.iters_out = s.iter + 1;
+    } else {
+      bool finish = fval <= qval;
+      if (!finish) {
+        s.c *= kEta;
+        s.trial += 1;
+        finish = s.trial >= p.maxiter || s.c > 1.0e200;
+      }
+      if (finish) {
+        s.c /= kEta;
+        const double mu = s.mu;
+        const double munew = (1 + sqrt(1 + 4 * mu * mu)) / 2;
+        fval += p.lambda_l1 * tot[kQL1];
+        if (fval < s.cost[s.iter % kCostRing]) {
+          s.cost_now = fval;
+          s.mom_a = (1 - mu) / munew;
+          s.mom_b = 1 + ((mu - 1) / munew);
+          s.take_x = 1;
+          s.l1x = tot[kQL1];
+        } else {
+          s.mom_a = 1 - (mu / munew);
+          s.mom_b = mu / munew;
+          s.take_x = 0;
+        }
+        s.accepted = 1;
+        bool stop = s.iter >= kMinIter && (s.cost[(s.iter - kTD) % kCostRing] - s.cost[s.iter % kCostRing]) < p.eps;
+        if (!stop && p.target > 0 && s.cost_now <= p.target) stop = true;
+        if (stop) {
+          s.active = 0;
+          s.iters_out = s.iter + 1;
+        } else {
+          s.mu = munew;
+          s.iter += 1;
+          if (s.iter >= p.maxiter) {
+            s.active = 0;
+            s.iters_out = p.maxiter;
+          } else {
+            s.need_grad = 1;
+          }
+        }
+      }
+    }
+  }
+  for (int k = 0; k < (int)gridDim.x; ++k) st[k] = s;
+  __threadfence();
+  if (set_handle) cudaGraphSetConditional(handle, s.active ? 1u : 0u);
+  if (any_active) *any_active = s.active;
+  if (cfg.mode == kCtrlStep && cfg.steps) cfg.steps[0] += 1ull;
+  *ticket = 0u;
 }
 
 // One CTA per problem.  The four warps reduce the partial sums (fixed order),
@@ -252,11 +414,16 @@ __global__ void __launch_bounds__(128) k_control(const ProbParams* __restrict__ 
       bool need = q == kQChiX || q == kQL1 || q == kQReg;
       if (cfg.mode == kCtrlStep) need = need || q == kQChiZ || q == kQTsvZ || q == kQDq1 || q == kQDq2;
       if (cfg.mode == kCtrlFinal) need = need || q == kQNact;
+      if (cfg.joint) need = need || (q == kQDtX) || (cfg.mode == kCtrlStep && q == kQDtZ);
       double v = need ? warp_partial_sum(part.at(q, b), cfg.slots[q], lane) : 0.0;
       if (lane == 0) red[q] = v;
     }
   }
   __syncthreads();
+  if (cfg.joint && cfg.mode != kCtrlFinal) {
+    control_joint(prm, st, cfg, red, handle, set_handle, any_active, ticket);
+    return;
+  }
   if (threadIdx.x == 0) {
     ProbState s = st[b];
     const ProbParams p = prm[b];
@@ -358,6 +525,7 @@ __global__ void __launch_bounds__(128) k_control(const ProbParams* __restrict__ 
       else if (rk == 2) fc += p.lambda_tv * reg;
       o.finalcost = fc;
       o.lip = s.c;
+      o.dt_pair = cfg.joint ? red[kQDtX] : 0.0;
       o.iters = s.iters_out;
       o.status = s.status;
       out[b] = o;

@@ -1015,6 +1015,20 @@ struct Solver {
   int per_step_launches = 0;
   int fixed_launches = 0;
   int ref_block_launches = 0, grad_block_launches = 0, rest_launches = 0;
+  // movie mode (set_movie before finish_setup): the B problems are the
+  // frames of one problem coupled by lam_t sum_b |x_b - x_{b+1}|^2 wt_b
+  bool joint = false;
+  double lam_t = 0.0;
+  DevMem d_wt, d_jq;
+
+  void set_movie(const std::vector<double>& wt, double lam) {
+    joint = true;
+    lam_t = lam;
+    std::vector<double> w(wt);
+    if (w.empty()) w.push_back(0.0);
+    d_wt.upload(w.data(), w.size());
+    d_jq.alloc(sizeof(double) * (size_t)ctx.B * kNumQ);
+  }
   // device loop with conditional IF blocks: the refresh and gradient blocks
   // run only in steps where some problem needs them (k_select_blocks)
   bool cond_blocks = false;
@@ -1090,10 +1104,10 @@ struct Solver {
     // kernels per loop step: the anchor refresh block, the gradient block
     // and the rest (trial point, its forward pass, control, momentum)
     ref_block_launches = op->corrected() ? 1 + op->launches_refresh() : 0;
-    grad_block_launches = (op->models_z() ? 1 : op->launches_forward()) + op->launches_adjoint();
-    rest_launches = op->launches_forward() + 3 + (form == kFormTV ? 1 : 0) + (op->models_z() ? 1 : 0);
+    grad_block_launches = (op->models_z() ? 1 : op->launches_forward()) + op->launches_adjoint() + (joint ? 1 : 0);
+    rest_launches = op->launches_forward() + 3 + (form == kFormTV ? 1 : 0) + (op->models_z() ? 1 : 0) + (joint ? 1 : 0);
     per_step_launches = ref_block_launches + grad_block_launches + rest_launches;
-    fixed_launches = 2 * (op->launches_forward() + 2) + 1;
+    fixed_launches = 2 * (op->launches_forward() + 2) + 1 + (joint ? 2 : 0);
     const char* hl = getenv("MFISTA_HOST_LOOP");
     host_loop = hl && hl[0] == '1';
     build_graph();
@@ -1219,6 +1233,11 @@ struct Solver {
     // objective the forms are held to, and MFISTA's monotone rule still
     // keeps x whenever F(xnew) rises
     cfg.bt_slack = refresh_every > 0 ? 1e-9 : 0.0;
+    cfg.joint = joint ? 1 : 0;
+    cfg.lam_t = lam_t;
+    cfg.jq = d_jq.as<double>();
+    cfg.slots[kQDtZ] = joint ? img_blocks() : 0;
+    cfg.slots[kQDtX] = joint ? img_blocks() : 0;
     return cfg;
   }
 
@@ -1282,12 +1301,20 @@ struct Solver {
       // the adjoint folds in the TSV gradient of z; TSV(z) itself is reduced by
       // k_update_tsv with the same tree as TSV(xnew)
       op->adjoint(bs, form == kFormTSV ? ctx.z : nullptr, -1);
+      if (joint) {  // temporal gradient and term at z
+        k_movie_tgrad<<<ig, 256, 0, bs>>>(ctx.z, ctx.dfdx, dm, d_wt.as<double>(), lam_t, ctx.st, ctx.part);
+        MF_LAUNCH_CK();
+      }
       if (cond) end_if();
     }
     // trial point
     if (form == kFormTSV) {
       k_update_tsv<<<ig, 256, 0, s>>>(ctx.z, ctx.dfdx, ctx.xnew, dm, ctx.prm, ctx.st, box_ptr, ctx.part);
       MF_LAUNCH_CK();
+      if (joint) {
+        k_movie_dx<<<ig, 256, 0, s>>>(ctx.xnew, dm, d_wt.as<double>(), ctx.st, kGateTrial, ctx.part);
+        MF_LAUNCH_CK();
+      }
     } else {
       launch_fgp(s);
       k_stats<<<ig, 256, 0, s>>>(ctx.xnew, ctx.z, ctx.dfdx, dm, ctx.prm, ctx.st, kGateTrial, form, 0, 1, ctx.part);
@@ -1531,6 +1558,10 @@ struct Solver {
       op->forward_exact(stream, ctx.x, kGateInit, kQChiX, false);
       k_stats<<<ig, 256, 0, stream>>>(ctx.x, nullptr, nullptr, dm, ctx.prm, ctx.st, kGateInit, form, 0, 0, ctx.part);
       MF_LAUNCH_CK();
+      if (joint) {
+        k_movie_dx<<<ig, 256, 0, stream>>>(ctx.x, dm, d_wt.as<double>(), ctx.st, kGateInit, ctx.part);
+        MF_LAUNCH_CK();
+      }
       launch_control(stream, kCtrlInit, 0, 0);
       if (!host_loop) {
         MF_CK(cudaGraphLaunch(exec, stream));
@@ -1546,6 +1577,10 @@ struct Solver {
     op->forward_exact(stream, ctx.x, kGateAll, kQChiX, true);
     k_stats<<<ig, 256, 0, stream>>>(ctx.x, nullptr, nullptr, dm, ctx.prm, ctx.st, kGateAll, form, 1, 0, ctx.part);
     MF_LAUNCH_CK();
+    if (joint) {
+      k_movie_dx<<<ig, 256, 0, stream>>>(ctx.x, dm, d_wt.as<double>(), ctx.st, kGateAll, ctx.part);
+      MF_LAUNCH_CK();
+    }
     launch_control(stream, kCtrlFinal, 0, 0);
   }
 
