@@ -226,7 +226,7 @@ int mfista_plan_set_shapes(mfista_plan plan, const int *shapes);
  * plan's kernels in isolation (as mfista_plan_profile, `reps` launches),
  * one knob at a time, both with every problem active (t_all) and with one
  * problem active (t_one, the tail of a batched solve), keeps the shape
- * minimising t_all / min t_all + t_one / min t_one, and captures the graph
+ * minimising t_all / min t_all + 2 t_one / min t_one, and captures the graph
  * again.  shapes_out: int[4] chosen shapes; ms_out: double[4] t_all per
  * launch of each knob's kernels at the chosen shape (0 for unused knobs).
  * Either may be NULL.  Like mfista_plan_profile, it leaves the iterates

@@ -1351,8 +1351,10 @@ struct Solver {
   // launch shapes that spread one problem over more CTAs win, so every
   // candidate is timed twice: with the whole batch active (t_all) and with
   // one problem active (t_one).  The choice minimises
-  // t_all / min t_all + t_one / min t_one.  ms_out[k]: t_all (ms per launch)
-  // of knob k's choice.
+  // t_all / min t_all + 2 t_one / min t_one: a lambda grid's iteration
+  // counts spread over decades, so many loop steps run with a handful of
+  // problems left (the 128x128 64-problem grid: 2234 of 4553 steps with 8
+  // or fewer).  ms_out[k]: t_all (ms per launch) of knob k's choice.
   LaunchShapes tune(int reps, double ms_out[4]) {
     LaunchShapes cur = op->shapes();
     // knob -> kernels timed (profile_kernel ids) and candidates
@@ -1397,7 +1399,7 @@ struct Solver {
         size_t best = 0;
         double best_score = 1e300;
         for (size_t i = 0; i < vals.size(); ++i) {
-          const double score = t_all[i] / ma + t_one[i] / m1;
+          const double score = t_all[i] / ma + 2.0 * t_one[i] / m1;
           if (score < best_score) {
             best_score = score;
             best = i;
