@@ -33,6 +33,7 @@ template <typename T> struct NufftGeom {
   const int* pt_hi;       // [B] one past its last point
   const int* tile_ptr;    // CSR over (geometry, tile): [ngeo*ntiles + 1]
   const int* tile_pts;    // point indices (global) binned to each tile
+  const int* tile_order;  // shared geometry: tiles by falling point count (launch order), or null
   int tile_bstride;       // ntiles, or 0 when all problems share one geometry
   long y2_bstride;        // per-problem offset of the residual, 0 if not shared
   const double* e4;       // [Nx*Ny] grid correction (shared by all problems)
@@ -962,7 +963,8 @@ __global__ void __launch_bounds__(256, SharedChunk<T>::kSpreadMinBlocks) k_nufft
   const int cnt = active_chunk<PB>(st, gate, B, blockIdx.y, sm.list, s_cnt);
   if (cnt == 0) return;  // uniform over the cluster: same problem chunk
   const int b0 = 0;
-  const int tile = blockIdx.x / csize;
+  // densest tiles first, so that the longest clusters start in the first wave
+  const int tile = geo.tile_order ? geo.tile_order[blockIdx.x / csize] : blockIdx.x / csize;
   // accumulator slot i holds problem b0 + list[i]: the smallest unrolled
   // width that holds the chunk's active problems
   if (cnt == 1)

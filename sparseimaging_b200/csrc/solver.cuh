@@ -240,6 +240,7 @@ template <typename T> struct NufftOp : Op {
   DevMem d_ax, d_axn, d_az;                // models of x, the trial point and z [y2 layout]
   bool model = false;                      // forward at z by linearity (corrected form)
   DevMem d_u, d_v, d_mx, d_my, d_wx, d_wy, d_vr, d_vi, d_w, d_lo, d_hi, d_tptr, d_tpts, d_e4, d_grid, d_y2, tw2h;
+  DevMem d_tord;  // shared geometry: spreading tiles by falling point count
   FftHost<T> fh, fcol;
   NufftGeom<T> geo{};
   int rpc = 8, cpc = 8, tile_r = 8, tile_c = 32, ntiles = 0;
@@ -313,6 +314,13 @@ template <typename T> struct NufftOp : Op {
     }
     d_tptr.upload(tptr.data(), tptr.size());
     d_tpts.upload(tpts.data(), std::max<size_t>(tpts.size(), 1));
+    if (shared) {  // spreading launch order: tiles by falling point count (ties by index)
+      std::vector<int> ord(ntiles);
+      for (int t = 0; t < ntiles; ++t) ord[t] = t;
+      std::stable_sort(ord.begin(), ord.end(),
+                       [&](int a, int b) { return tptr[a + 1] - tptr[a] > tptr[b + 1] - tptr[b]; });
+      d_tord.upload(ord.data(), ord.size());
+    }
     // FFTs: rows as complex length Ny, columns length 2Nx
     fh.init(ny);
     fcol.init(2 * nx);
@@ -359,6 +367,7 @@ template <typename T> struct NufftOp : Op {
     geo.pt_hi = d_hi.as<int>();
     geo.tile_ptr = d_tptr.as<int>();
     geo.tile_pts = d_tpts.as<int>();
+    geo.tile_order = shared ? d_tord.as<int>() : nullptr;
     geo.tile_bstride = shared ? 0 : ntiles;
     geo.y2_bstride = shared ? mtot : 0;
     geo.e4 = d_e4.as<double>();
