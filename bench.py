@@ -7,14 +7,20 @@ solved for 64 (lambda_l1, lambda_tsv) pairs on an 8x8 log grid spanning
 its objective is within 1e-6 (relative) of F*, the FP64 optimum obtained
 beforehand (untimed) with the library's FP64 batched solver run long.
 
-One step = one batched solve of the 64 problems by the chosen method (all
-problems in one device-resident CUDA-graph loop, FP64, each stopping on its
-own at F* (1 + 1e-6)).  The FP32-operator form is run once more, untimed,
-and its accuracy against F* is reported beside the line.  The plain
-method (FP64, one problem per launch) is timed on the same targets as the
-comparison point.  Multi-GPU: every rank solves its own seeded lambda grid
-(no collective on the data path), value = all ranks' solves / max-over-ranks
-time (weak scaling).
+One step = one batched solve of the 64 problems by the chosen method
+(--method, default fp32: FP32 NUFFT/FFT operators with FP64 anchor
+correction and an FP64 objective; all problems in one device-resident
+CUDA-graph loop, each stopping on its own at F* (1 + 1e-6)).  The other
+precision is run once more, untimed, and both forms' accuracy against F*
+is reported beside the line.  The plain method (FP64, one problem per
+launch) is timed on the same targets as the comparison point, and the e2e
+figure repeats the chosen solve through mfista_nufft_batch from pinned host
+arrays.  Side measurements (untimed for `value`): the DFT lambda grid in
+FP64 and the tensor-core split-BF16 forms, the leave-one-out error of its
+solutions against a numpy/LAPACK host baseline, and a 48-frame movie batch.
+Multi-GPU: every rank solves its own seeded lambda grid (no collective on
+the data path), value = all ranks' solves / max-over-ranks time (weak
+scaling).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
