@@ -300,6 +300,14 @@ int mfista_dft_profile(const double *A, int M, int N, int B, int precision, int 
 int mfista_dft_looe(const double *y, const double *A, int M, int N, int NX, const double *X, int B,
                     const double *lambda_tsv, double *looe_m, double *looe_std, int *hessian_positive);
 
+/* Forward NUFFT of the reference's C++ build: x2y_nufft
+ * (c++/mfista_nufft_lib.cpp:1076-1149, exported by c++/mfista.hpp:136-137)
+ * with the same arguments, on the GPU in FP64: its 12-tap (MSP = 6) kernel,
+ * floor binning of points flipped to v >= 0 and Hermitian halo, which differ
+ * from the C library's operator (mfista_nufft_forward).  y_r, y_i: [M]. */
+int mfista_cpp_x2y_nufft(const double *u_dx, const double *v_dy, int M, int Nx, int Ny, const double *xin,
+                         double *y_r, double *y_i);
+
 /* FGP TV proximal map alone (FGP_L1_box / FGP_nonneg_box,
  * c/mfista_TV_lib.c:189-384) on an NX x NY view: x_out = prox(b). */
 int mfista_fgp_prox(const double *b, int NX, int NY, double lambda_l1, double lambda_tv,

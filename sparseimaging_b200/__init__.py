@@ -135,6 +135,8 @@ def lib():
         L.mfista_nufft_movie.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, C.c_int, C.c_int, C.c_int, _dp, C.c_double,
                                          C.c_double, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int, _dp,
                                          _dp, C.POINTER(RESULT), _dp]
+        L.mfista_cpp_x2y_nufft.restype = C.c_int
+        L.mfista_cpp_x2y_nufft.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]
         L.mfista_dft_looe.restype = C.c_int
         L.mfista_dft_looe.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp, _dp, _ip]
         L.mfista_plan_destroy.restype = None
@@ -383,6 +385,15 @@ def nufft_movie(u_dx, v_dy, vis_r, vis_i, vis_std, pt_off, nx, ny, lambda_l1, la
                                     _p(tl), lambda_l1, lambda_tsv, lambda_t, cinit, maxiter, eps, nonneg_flag,
                                     _p(xi), _p(xo), res, C.byref(tc)))
     return xo.reshape(T, nx * ny), [r.as_dict() for r in res], tc.value
+
+
+def cpp_x2y_nufft(u_dx, v_dy, nx, ny, x):
+    """Forward NUFFT of the reference's C++ build (x2y_nufft: 12-tap
+    kernel, floor binning) on the GPU; returns (real, imag)."""
+    u, v, xx = _d(u_dx), _d(v_dy), _d(x)
+    yr, yi = np.zeros(u.size), np.zeros(u.size)
+    _check(lib().mfista_cpp_x2y_nufft(_p(u), _p(v), u.size, nx, ny, _p(xx), _p(yr), _p(yi)))
+    return yr, yi
 
 
 def dft_looe(y, A, X, nx, lambda_tsv=None):

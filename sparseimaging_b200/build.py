@@ -16,7 +16,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libmfista_b200.so")
 SOURCES = ["mfista_b200.cu", "nufft_noalloc.cu", "unet.cu"]
 HEADERS = ["common.cuh", "fft_smem.cuh", "nufft_ops.cuh", "fftvar_ops.cuh", "dft_ops.cuh",
-           "mfista_ops.cuh", "fgp.cuh", "solver.cuh", "looe.cuh", "dft_tc.cuh"]
+           "mfista_ops.cuh", "fgp.cuh", "solver.cuh", "looe.cuh", "dft_tc.cuh", "cpp_nufft.cuh"]
 
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared", "-cudart", "static"]

@@ -8,6 +8,7 @@
 
 #include "solver.cuh"
 #include "looe.cuh"
+#include "cpp_nufft.cuh"
 
 using namespace mf;
 
@@ -810,6 +811,52 @@ extern "C" int mfista_nufft_movie(const double* u_dx, const double* v_dy, const 
                     false, cinit);
       }
     if (o[0].status) return fail(o[0].status, "the movie stopped early (status " + std::to_string(o[0].status) + ")", false);
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
+// forward NUFFT of the reference's C++ build (x2y_nufft), see cpp_nufft.cuh
+extern "C" int mfista_cpp_x2y_nufft(const double* u_dx, const double* v_dy, int M, int Nx, int Ny, const double* xin,
+                                    double* y_r, double* y_i) {
+  set_ok();
+  try {
+    if (M < 1 || Nx < 12 || Ny < 12) throw Error(MFISTA_ERR_ARG, "mfista_cpp_x2y_nufft: needs M >= 1, Nx, Ny >= 12");
+    if (!u_dx || !v_dy || !xin || !y_r || !y_i) throw Error(MFISTA_ERR_ARG, "mfista_cpp_x2y_nufft: null pointer");
+    cppnufft::Prep pr(u_dx, v_dy, M, Nx, Ny);
+    Solver S;
+    S.precision = MFISTA_FP64;
+    S.init_common(1, Nx * Ny, Nx, Ny, kFormTSV, 100, nullptr);
+    std::vector<double> zero(M, 0.0), one(M, 1.0);
+    NufftInput in{u_dx, v_dy, zero.data(), zero.data(), one.data(), nullptr, 1, M, Nx, Ny};
+    NufftOp<double>* op = new NufftOp<double>(S.ctx, in);
+    S.op.reset(op);
+    ProbState st;
+    memset(&st, 0, sizeof(st));
+    st.active = 1;
+    MF_CK(cudaMemcpyAsync(S.ctx.st, &st, sizeof(st), cudaMemcpyHostToDevice, S.stream));
+    op->d_e4.upload(pr.e4.data(), pr.e4.size());  // the C++ build's grid correction
+    op->geo.e4 = op->d_e4.as<double>();
+    MF_CK(cudaMemcpyAsync(S.ctx.x, xin, sizeof(double) * (size_t)Nx * Ny, cudaMemcpyHostToDevice, S.stream));
+    op->launch_rows_fwd(S.stream, S.ctx.x, kGateAll, nullptr);
+    op->launch_cols_fwd(S.stream, kGateAll);
+    DevMem d_mx, d_my, d_yn, d_e1, d_e2x, d_e2y, d_out;
+    d_mx.upload(pr.mx.data(), M);
+    d_my.upload(pr.my.data(), M);
+    d_yn.upload(pr.yneg.data(), M);
+    d_e1.upload(pr.e1.data(), M);
+    d_e2x.upload(pr.e2x.data(), pr.e2x.size());
+    d_e2y.upload(pr.e2y.data(), pr.e2y.size());
+    d_out.alloc(sizeof(double) * 2 * (size_t)M);
+    cppnufft::k_cpp_interp<<<cdiv(M, 8), 256, 0, S.stream>>>(
+        op->d_grid.as<cplx<double>>(), Nx, Ny, d_mx.as<int>(), d_my.as<int>(), d_yn.as<int>(), d_e1.as<double>(),
+        d_e2x.as<double>(), d_e2y.as<double>(), M, 1.0 / (4.0 * (double)Nx * (double)Ny), d_out.as<double>(),
+        d_out.as<double>() + M);
+    MF_LAUNCH_CK();
+    MF_CK(cudaMemcpyAsync(y_r, d_out.p, sizeof(double) * M, cudaMemcpyDeviceToHost, S.stream));
+    MF_CK(cudaMemcpyAsync(y_i, d_out.as<double>() + M, sizeof(double) * M, cudaMemcpyDeviceToHost, S.stream));
+    MF_CK(cudaStreamSynchronize(S.stream));
     return MFISTA_OK;
   } catch (const Error& e) {
     return fail(e.status, e.what(), false);
