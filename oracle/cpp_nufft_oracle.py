@@ -123,3 +123,34 @@ class CppNufftPlan:
         C[nx:] = L[MSP:MSP + nx, MSP:MSP + ny + 1]
         out = np.fft.irfft2(C, s=(2 * nx, 2 * ny)) * (4.0 * nx * ny)
         return (out[np.ix_(self.pr, self.pc)] * self.e4).ravel()
+
+
+def cpp_imaging_core_nufft(u_dx, v_dy, vis_r, vis_i, vis_std, nx, ny, maxiter, eps, lam_l1, lam_tsv, cinit,
+                           xinit, nonneg_flag):
+    """The C++ build's mfista_imaging_core_nufft, TSV form
+    (c++/mfista_nufft_lib.cpp:680-929, :1016-1074): the C library's loop
+    with these operators and a backtracking factor of 10 in the first
+    iteration.  Returns (xout, iterations, final c).  The C++ build also
+    sorts the caller's u, v, vis arrays in place (sort_input :550-641); the
+    sums here do not depend on the order beyond rounding, so it is left
+    out.  eps is scaled as in the C library (:1031-1034)."""
+    from . import mfista_oracle as R
+    vis_r = np.asarray(vis_r, np.float64)
+    vis_i = np.asarray(vis_i, np.float64)
+    m = vis_r.size
+    epsilon = (vis_r @ vis_r + vis_i @ vis_i) * eps / float(m)
+    plan = CppNufftPlan(u_dx, v_dy, nx, ny)
+    w = 1.0 / np.asarray(vis_std, np.float64)
+
+    def f_part(x):
+        fr, fi = plan.forward(x)
+        rr = (vis_r - fr) * w
+        ri = (vis_i - fi) * w
+        return 0.5 * (rr @ rr + ri @ ri), (rr, ri)
+
+    def grad(res):
+        rr, ri = res
+        return plan.adjoint(rr * w, ri * w)
+
+    return R.mfista(f_part, grad, xinit, nx, ny, maxiter, epsilon, lam_l1, 0.0, lam_tsv, cinit, nonneg_flag,
+                    eta_first=10.0)

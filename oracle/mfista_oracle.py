@@ -376,12 +376,15 @@ def q_part(xnew, z, c, dfdx):
 # --------------------------------------------------------------------------
 
 def mfista(f_part, grad, x0, nx, ny, maxiter, eps, lam_l1, lam_tv, lam_tsv, cinit,
-           nonneg_flag, box_flag=0, cl_box=None, fgp_iter=FGPITER, trace=None):
+           nonneg_flag, box_flag=0, cl_box=None, fgp_iter=FGPITER, trace=None, eta_first=None):
     """Returns (xout, iterations, c).  ``eps`` is the already-scaled threshold.
 
     TSV form when lam_tv == 0, TV form otherwise (the caller checks the
     both-positive error case).  ``trace`` (a list) collects per-iteration
-    (cost, c) pairs when given."""
+    (cost, c) pairs when given.  ``eta_first``: the backtracking factor of
+    the first outer iteration only (the C++ build uses 10,
+    c++/mfista_nufft_lib.cpp:818, :860-863; the C library ETA throughout);
+    the division after every backtracking loop stays ETA."""
     use_tv = lam_tv != 0
     box = np.asarray(cl_box) if box_flag == 1 else None
     x = np.array(x0, dtype=np.float64, copy=True)
@@ -431,7 +434,7 @@ def mfista(f_part, grad, x0, nx, ny, maxiter, eps, lam_l1, lam_tv, lam_tsv, cini
             qval = q_part(xnew, z, c, dfdx) + qcore
             if fval <= qval:
                 break
-            c *= ETA
+            c *= ETA if (eta_first is None or it > 0) else eta_first
         c /= ETA
         munew = (1 + math.sqrt(1 + 4 * mu * mu)) / 2
         fval += lam_l1 * np.abs(xnew).sum()
