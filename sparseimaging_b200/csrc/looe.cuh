@@ -266,13 +266,12 @@ __global__ void k_looe_final(const double* __restrict__ part, int nblk, int M, c
 }
 
 // Host driver: LOOE of B solutions X [B][N] of the DFT problem (y [M], A
-// column-major M x N); lambda_tsv per solution (null: 0).  Launch counts per
-// solution: 5 (+1 TSV) + ceil(n_s/64) x (up to 5) kernels.
+// column-major M x N); lambda_tsv per solution (null: 0).  Kernels per
+// solution: 5 (+1 TSV) + ceil(n_s/64) x (up to 5).
 struct Looe {
   int M, N, NX;
   cudaStream_t s = nullptr;
   DevMem d_A, d_y, d_S, d_xs, d_r, d_Z, d_H, d_part, d_info, d_out;
-  long long launches = 0;
 
   Looe(const double* y, const double* A, int M_, int N_, int NX_) : M(M_), N(N_), NX(NX_) {
     MF_CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -294,7 +293,6 @@ struct Looe {
     k_looe_gemm<TA, TB><<<dim3(cdiv(m, kGT), cdiv(n, kGT)), 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C,
                                                                           ldc, lower, d_info.as<int>());
     MF_LAUNCH_CK();
-    ++launches;
   }
 
   // (looe_m, looe_std, positive) of one solution x [N]
@@ -320,16 +318,13 @@ struct Looe {
     k_looe_resid<<<cdiv(M, 256), 256, 0, s>>>(d_A.as<double>(), M, d_y.as<double>(), d_S.as<int>(),
                                                 d_xs.as<double>(), ns, d_r.as<double>());
     MF_LAUNCH_CK();
-    ++launches;
     if (ns > 0) {
       k_looe_gather<<<ns, 256, 0, s>>>(d_A.as<double>(), M, d_S.as<int>(), Z);
       MF_LAUNCH_CK();
-      ++launches;
       gemm<true, false>(ns, ns, M, 1.0, Z, M, Z, M, 0.0, H, ns, 1);  // H = Z^T Z
       if (lam_tsv != 0.0) {
         k_looe_tsv_diag<<<cdiv(ns, 256), 256, 0, s>>>(H, ns, d_S.as<int>(), ns, NX, lam_tsv);
         MF_LAUNCH_CK();
-        ++launches;
       }
       for (int k0 = 0; k0 < ns; k0 += kPanel) {
         const int nb = std::min(kPanel, ns - k0), k1 = k0 + nb, rem = ns - k1;
@@ -346,7 +341,6 @@ struct Looe {
         // Z[:, k0:k1] := Z[:, k0:k1] L_kk^-T, then Z[:, k1:] -= Z[:, k0:k1] L21^T
         k_looe_rowsolve<<<cdiv(M, 256), 256, 0, s>>>(Z + (size_t)k0 * M, M, 0, M, Ld, ns, nb, info);
         MF_LAUNCH_CK();
-        launches += 2 + (rem > 0 ? 1 : 0);  // diagonal, row solves (the GEMMs count themselves)
         if (rem > 0)
           gemm<false, true>(M, rem, nb, -1.0, Z + (size_t)k0 * M, M, H + k1 + (size_t)k0 * ns, ns, 1.0,
                             Z + (size_t)k1 * M, M, 0);
@@ -357,7 +351,6 @@ struct Looe {
     MF_LAUNCH_CK();
     k_looe_final<<<1, 32, 0, s>>>(d_part.as<double>(), nblk, M, info, d_out.as<double>());
     MF_LAUNCH_CK();
-    launches += 2;
     MF_CK(cudaMemcpyAsync(out, d_out.p, sizeof(double) * 3, cudaMemcpyDeviceToHost, s));
     MF_CK(cudaStreamSynchronize(s));
   }
