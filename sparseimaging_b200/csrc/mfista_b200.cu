@@ -274,6 +274,11 @@ extern "C" mfista_plan mfista_nufft_plan_create(const double* u_dx, const double
     if (B < 1) throw Error(MFISTA_ERR_ARG, "B must be >= 1");
     if (precision != MFISTA_FP32 && precision != MFISTA_FP64) throw Error(MFISTA_ERR_ARG, "precision must be 32 or 64");
     if (!shared_geometry && !pt_off) throw Error(MFISTA_ERR_ARG, "pt_off required without shared geometry");
+    if (!shared_geometry) {
+      if (pt_off[0] < 0) throw Error(MFISTA_ERR_ARG, "pt_off[0] must be >= 0");
+      for (int b = 0; b < B; ++b)
+        if (pt_off[b + 1] < pt_off[b]) throw Error(MFISTA_ERR_ARG, "pt_off must not decrease");
+    }
     std::unique_ptr<mfista_plan_s> P(new mfista_plan_s);
     P->B = B;
     P->Nx = Nx;
@@ -773,6 +778,9 @@ extern "C" int mfista_nufft_movie(const double* u_dx, const double* v_dy, const 
     if (maxiter < 0) throw Error(MFISTA_ERR_ARG, "maxiter must be >= 0");
     if (nonneg_flag != 0 && nonneg_flag != 1) throw Error(MFISTA_ERR_ARG, "nonneg_flag must be 0 or 1");
     if (lambda_t < 0 || lambda_tsv < 0) throw Error(MFISTA_ERR_ARG, "lambda_t and lambda_tsv must be >= 0");
+    if (pt_off[0] < 0) throw Error(MFISTA_ERR_ARG, "pt_off[0] must be >= 0");
+    for (int b = 0; b < n_frames; ++b)
+      if (pt_off[b + 1] < pt_off[b]) throw Error(MFISTA_ERR_ARG, "pt_off must not decrease");
     std::vector<double> wt(std::max(n_frames - 1, 0));
     for (int b = 0; b + 1 < n_frames; ++b) {
       const double dt = t_list ? t_list[b + 1] - t_list[b] : 1.0;
