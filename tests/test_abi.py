@@ -104,3 +104,20 @@ def test_python_binding_raises_without_library(monkeypatch, tmp_path):
     monkeypatch.setattr(si, "_lib", None)
     with pytest.raises(RuntimeError):
         si.lib()
+
+
+def test_cpp_build_shim_links(tmp_path):
+    """The one-line shim INTEGRATION.md gives programs written against the
+    reference's C++ build (x2y_nufft, c++/mfista.hpp:136-137) compiles
+    against our header and links against the library (nothing is run)."""
+    from sparseimaging_b200 import build
+    src = tmp_path / "shim.c"
+    src.write_text('#include "%s"\n' % HEADER + r"""
+void x2y_nufft(double *u_dx, double *v_dy, int M, int Nx, int Ny,
+               double *xin, double *y_r, double *y_i)
+{ mfista_cpp_x2y_nufft(u_dx, v_dy, M, Nx, Ny, xin, y_r, y_i); }
+int main(int argc, char **argv) { if (argc > 99) x2y_nufft(0, 0, 0, 0, 0, 0, 0, 0); return 0; }
+""")
+    libdir = os.path.dirname(build.LIB)
+    subprocess.run(["gcc", "-Werror", "-o", str(tmp_path / "shim"), str(src), f"-L{libdir}",
+                    f"-l:{os.path.basename(build.LIB)}", f"-Wl,-rpath,{libdir}"], check=True)
