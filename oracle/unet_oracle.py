@@ -3,7 +3,7 @@
 A float64 numpy restatement of the network that `csrc/unet.cu` trains on
 the GPU, with its forward pass, loss and backward pass, used to check the
 GPU kernels' outputs and parameter gradients.  The reference has no such
-network (it is the learned warm start of the north star); what is restated
+network (it is this library's learned warm start); what is restated
 here is the architecture and the parameter layout of `csrc/unet.cu`:
 
   e1a = relu(conv(x, 2->16)),  e1 = relu(conv(e1a, 16->16))           H

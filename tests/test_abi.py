@@ -107,9 +107,9 @@ def test_python_binding_raises_without_library(monkeypatch, tmp_path):
 
 
 def test_cpp_build_shim_links(tmp_path):
-    """The one-line shim INTEGRATION.md gives programs written against the
-    reference's C++ build (x2y_nufft, c++/mfista.hpp:136-137) compiles
-    against our header and links against the library (nothing is run)."""
+    """A one-line shim that gives programs written against the reference's
+    C++ build its x2y_nufft (c++/mfista.hpp:136-137) compiles against our
+    header and links against the library (nothing is run)."""
     from sparseimaging_b200 import build
     src = tmp_path / "shim.c"
     src.write_text('#include "%s"\n' % HEADER + r"""
