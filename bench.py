@@ -17,7 +17,8 @@ launch) is timed on the same targets as the comparison point, and the e2e
 figure repeats the chosen solve through mfista_nufft_batch from pinned host
 arrays.  Side measurements (untimed for `value`): the DFT lambda grid in
 FP64 and the tensor-core split-BF16 forms, the leave-one-out error of its
-solutions against a numpy/LAPACK host baseline, and a 48-frame movie batch.
+solutions against a numpy/LAPACK host baseline, a 48-frame movie batch and
+the same frames solved as one movie with the temporal term.
 Multi-GPU: every rank solves its own seeded lambda grid (no collective on
 the data path), value = all ranks' solves / max-over-ranks time (weak
 scaling).
@@ -181,7 +182,36 @@ def movie_batch(si):
             "fp32": {"frames_per_s": round(len(frames) / R32[0]["comp_time"], 3),
                      "mean_iters": float(np.mean([r["ITER"] for r in R32]))},
             "fp32_vs_fp64_rel_objective": {"median": float(np.median(dobj)), "max": float(max(dobj))},
-            "fp32_vs_fp64_rel_image": {"median": float(np.median(dimg)), "max": float(max(dimg))}}
+            "fp32_vs_fp64_rel_image": {"median": float(np.median(dimg)), "max": float(max(dimg))},
+            "joint": _reported(movie_joint, si, geo, off, probs)}
+
+
+def _reported(fn, *args):
+    """fn(*args), or its error as a short record (side measurements are
+    reported, not required)."""
+    try:
+        return fn(*args)
+    except Exception as e:
+        return {"error": str(e)[:200]}
+
+
+def movie_joint(si, geo, off, probs):
+    """The same 48 frames solved as ONE movie (mfista_nufft_movie, FP64):
+    one lambda (the frames' median), temporal weight lambda_t = 5 lambda
+    and 0 (uncoupled frames under one step size), 1000 iterations each;
+    time per solve and the temporal term sum_b |x_b - x_{b+1}|^2 it
+    leaves."""
+    lam = float(np.median([q["lambda_l1"] for q in probs]))
+    lip = float(max(q["cinit"] for q in probs))
+    out = {"frames": len(probs), "iterations": 1000, "lambda_t_over_lambda": 5.0}
+    for name, lt in (("coupled", 5.0 * lam), ("uncoupled", 0.0)):
+        X, R, tcost = si.nufft_movie(*geo[:5], off, geo[5], geo[6], lam, 1e-3 * lam, lt, lip, 1000, 0.0)
+        D = X[:-1] - X[1:]
+        out[name] = {"solve_s": round(R[0]["comp_time"], 4),
+                     "iterations_per_s": round(R[0]["ITER"] / R[0]["comp_time"], 1),
+                     "temporal_sum": float(np.sum(D * D)),
+                     "objective": float(sum(r["finalcost"] for r in R) + tcost)}
+    return out
 
 
 def workload_name(nx, m, b):
