@@ -185,6 +185,22 @@ int mfista_dft_batch(const double *y, const double *A, int M, int N, int NX, int
                      const struct mfista_problem *problems, double eps, int precision,
                      int fgp_iter, const double *xinit, double *xout, struct RESULT *results);
 
+/* Batched FFT (gridded) variant: B problems sharing the gridded data of
+ * mfista_imaging_core_fft (u_idx, v_idx, y_r, y_i, noise_stdev [M] on an
+ * NX x NY grid, e.g. a lambda grid) advance together, each with its own
+ * backtracking state and convergence mask.  eps is scaled as
+ * mfista_imaging_core_fft scales it (c/mfista_fft_lib.c:715-717).
+ * precision MFISTA_FP64, or MFISTA_FP32: FP32 FFTs and FGP stencils, the
+ * forward spectrum corrected by the exact FP64 spectrum of an anchor image
+ * refreshed every 32 outer iterations, objective / backtracking / FISTA
+ * sequence in FP64.  fgp_iter: FGP iterations of the TV form (the
+ * reference compiles in 100).  xinit: [B*NX*NY] or NULL; xout [B*NX*NY];
+ * results [B] (may be NULL).  No counterpart in the reference. */
+int mfista_fft_batch(const int *u_idx, const int *v_idx, const double *y_r, const double *y_i,
+                     const double *noise_stdev, int M, int NX, int NY, int B,
+                     const struct mfista_problem *problems, double eps, int precision, int fgp_iter,
+                     const double *xinit, double *xout, struct RESULT *results);
+
 /* Device-resident plan of a batched NUFFT solve.  Creation uploads the
  * geometry and visibilities once and builds the CUDA graph; mfista_plan_run
  * enqueues one whole batched solve on the plan's stream without waiting;
@@ -313,6 +329,14 @@ int mfista_cpp_x2y_nufft(const double *u_dx, const double *v_dy, int M, int Nx, 
 int mfista_fgp_prox(const double *b, int NX, int NY, double lambda_l1, double lambda_tv,
                     int iters, int nonneg_flag, int box_flag, const float *cl_box,
                     double *x_out, int precision);
+
+/* Times the FGP TV prox alone (the kernel mfista_fgp_prox runs) for B
+ * problems of NX x NY in one launch, `iters` FGP iterations each, in
+ * MFISTA_FP64 or MFISTA_FP32 stencil arithmetic: CUDA events around `reps`
+ * launches on the library's stream.  Outputs the mean milliseconds per
+ * launch and its compulsory bytes (image vectors read and written once). */
+int mfista_fgp_profile(int NX, int NY, int B, int iters, int precision, int reps, double *ms_per_launch,
+                       double *bytes_per_launch);
 
 /* Power-iteration estimate of the Lipschitz constant of the chi^2 gradient
  * (largest eigenvalue of A^H W^2 A) of a NUFFT problem, for choosing cinit. */

@@ -21,7 +21,7 @@ from .build import LIB
 
 __all__ = ["RESULT", "Problem", "MfistaError", "lib", "mfista_imaging_core_nufft",
            "mfista_imaging_core_fft", "mfista_imaging_core_dft", "imaging_core_nufft",
-           "imaging_core_fft", "imaging_core_dft", "nufft_batch", "dft_batch", "Plan", "nufft_forward",
+           "imaging_core_fft", "imaging_core_dft", "nufft_batch", "fft_batch", "fgp_profile", "dft_batch", "Plan", "nufft_forward",
            "nufft_adjoint", "fgp_prox", "nufft_lipschitz", "last_status", "last_error", "set_fgp_iter", "set_device",
            "dft_apply", "dft_profile", "FP64", "FP32", "BF16X3", "BF16X6"]
 
@@ -97,6 +97,12 @@ def lib():
         L.mfista_nufft_batch.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, C.c_int, C.c_int, C.c_int,
                                          C.c_int, C.c_int, C.POINTER(Problem), C.c_double, C.c_int,
                                          C.c_int, _dp, _dp, C.POINTER(RESULT)]
+        L.mfista_fft_batch.restype = C.c_int
+        L.mfista_fft_batch.argtypes = [_ip, _ip, _dp, _dp, _dp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.POINTER(Problem), C.c_double, C.c_int, C.c_int, _dp, _dp,
+                                       C.POINTER(RESULT)]
+        L.mfista_fgp_profile.restype = C.c_int
+        L.mfista_fgp_profile.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]
         L.mfista_dft_batch.restype = C.c_int
         L.mfista_dft_batch.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.POINTER(Problem), C.c_double, C.c_int, C.c_int, _dp, _dp,
@@ -316,6 +322,33 @@ def nufft_batch(u_dx, v_dy, vis_r, vis_i, vis_std, nx, ny, problems, eps, precis
                                   _p(xo), res)
     _check(st)
     return xo.reshape(B, n), [r.as_dict() for r in res]
+
+
+def fft_batch(u_idx, v_idx, y_r, y_i, noise, nx, ny, problems, eps, precision=FP64, xinit=None,
+              fgp_iter=100):
+    """Solves len(problems) FFT-variant problems sharing one gridded data
+    set (mfista_fft_batch); precision FP64 or FP32 (FP32 FFTs and FGP
+    stencils with an FP64-corrected forward spectrum)."""
+    ui = np.ascontiguousarray(u_idx, np.int32)
+    vi_ = np.ascontiguousarray(v_idx, np.int32)
+    yr, yi, ns = (_d(a) for a in (y_r, y_i, noise))
+    B = len(problems)
+    n = nx * ny
+    xi = None if xinit is None else _d(xinit)
+    xo = np.zeros(B * n)
+    res = (RESULT * B)()
+    st = lib().mfista_fft_batch(_p(ui, _ip), _p(vi_, _ip), _p(yr), _p(yi), _p(ns), ui.size, nx, ny, B,
+                                _problems(problems), eps, precision, fgp_iter, _p(xi), _p(xo), res)
+    _check(st)
+    return xo.reshape(B, n), [r.as_dict() for r in res]
+
+
+def fgp_profile(nx, ny, B, iters, precision=FP64, reps=10):
+    """(ms per launch, compulsory bytes per launch) of the FGP TV prox for B
+    problems of nx x ny with `iters` FGP iterations (mfista_fgp_profile)."""
+    ms, by = C.c_double(), C.c_double()
+    _check(lib().mfista_fgp_profile(nx, ny, B, iters, precision, reps, C.byref(ms), C.byref(by)))
+    return ms.value, by.value
 
 
 def dft_batch(y, A, nx, ny, problems, eps, xinit=None, fgp_iter=100, precision=None):

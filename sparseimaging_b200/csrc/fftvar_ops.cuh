@@ -18,11 +18,14 @@ struct FftVarGeom {
   long geo_stride;
 };
 
-// real FFT of every image row (length NY as NY/2 complex points)
+// real FFT of every image row (length NY as NY/2 complex points); with
+// `sub` (the FP64 anchor images of the corrected FP32 form) the rows of
+// x - sub are transformed
 template <typename T>
 __global__ void k_fftv_rows_fwd(const double* __restrict__ xall, long xstride, cplx<T>* __restrict__ hall,
                                 long hstride, int nx, int ny, FftDev<T> fh, const cplx<T>* __restrict__ tw2h,
-                                const ProbState* __restrict__ st, int gate, int rows_per_cta) {
+                                const ProbState* __restrict__ st, int gate, int rows_per_cta,
+                                const double* __restrict__ suball) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   int b = blockIdx.y;
   if (!gate_ok(st[b], gate)) return;
@@ -33,10 +36,16 @@ __global__ void k_fftv_rows_fwd(const double* __restrict__ xall, long xstride, c
   cplx<T>* H = hall + (size_t)b * hstride;
   int i0 = blockIdx.x * rows_per_cta;
   int nrows = min(rows_per_cta, nx - i0);
+  const double* sub = suball ? suball + (size_t)b * xstride : nullptr;
   for (int t = threadIdx.x; t < nrows * h; t += blockDim.x) {
     int rr = t / h, m = t - rr * h;
-    const double* xr = x + (size_t)(i0 + rr) * ny;
-    A[rr * ld + m] = mk<T>((T)xr[2 * m], (T)xr[2 * m + 1]);
+    const size_t f = (size_t)(i0 + rr) * ny + 2 * m;
+    double x0 = x[f], x1 = x[f + 1];
+    if (sub) {
+      x0 -= sub[f];
+      x1 -= sub[f + 1];
+    }
+    A[rr * ld + m] = mk<T>((T)x0, (T)x1);
   }
   __syncthreads();
   cplx<T>* Z = smem_fft<T>(A, Bf, fh, ld, nrows, -1);
@@ -52,11 +61,15 @@ __global__ void k_fftv_rows_fwd(const double* __restrict__ xall, long xstride, c
 
 // column FFT (length NX) over the half spectrum; forward pass fuses
 // calc_yAx_fft (:116-130), the weighted norm and, in gradient mode, the
-// mask / (2 sqrt N) scaling of dF_dx_fft (:170).
+// mask / (2 sqrt N) scaling of dF_dx_fft (:170).  Corrected FP32 form: the
+// spectrum is base + FFT(x - x_a) with base the exact FP64 spectrum of the
+// anchor (added in FP64 before the residual); raw_out (forward, qchi < 0)
+// stores the FP64 spectrum itself (the anchor refresh of the exact operator).
 template <typename T>
 __global__ void k_fftv_cols(cplx<T>* __restrict__ hall, long hstride, int nx, int nyh, FftDev<T> fnx, int sign,
                             int cols_per_cta, FftVarGeom geo, double sqrtn, const ProbState* __restrict__ st,
-                            int gate, Partials part, int qchi, int store_grad) {
+                            int gate, Partials part, int qchi, int store_grad, const double2* __restrict__ base,
+                            double2* __restrict__ raw_out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double sh[32];
   int b = blockIdx.y;
@@ -83,11 +96,19 @@ __global__ void k_fftv_cols(cplx<T>* __restrict__ hall, long hstride, int nx, in
     int k = c0 + cc;
     size_t e = (size_t)r * nyh + k;
     cplx<T> v = R[cc * ld + r];
-    if (qchi >= 0) {
+    if (raw_out) {
+      raw_out[(size_t)b * hstride + e] = make_double2((double)v.x, (double)v.y);
+    } else if (qchi >= 0) {
       double mk_ = mask[e];
       double2 y = yf[e];
-      double rr = y.x - mk_ * (double)v.x / sqrtn;
-      double ri = y.y - mk_ * (double)v.y / sqrtn;
+      double vx = (double)v.x, vy = (double)v.y;
+      if (base) {
+        const double2 a = base[(size_t)b * hstride + e];
+        vx += a.x;
+        vy += a.y;
+      }
+      double rr = y.x - mk_ * vx / sqrtn;
+      double ri = y.y - mk_ * vy / sqrtn;
       double w = (k == 0 || k == nyh - 1) ? 1.0 : 2.0;
       acc[0] += w * (rr * rr + ri * ri);
       if (store_grad) {

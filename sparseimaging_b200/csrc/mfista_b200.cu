@@ -521,6 +521,63 @@ extern "C" int mfista_dft_batch(const double* y, const double* A, int M, int N, 
   }
 }
 
+extern "C" int mfista_fft_batch(const int* u_idx, const int* v_idx, const double* y_r, const double* y_i,
+                                const double* noise_stdev, int M, int NX, int NY, int B,
+                                const struct mfista_problem* problems, double eps, int precision, int fgp_iter,
+                                const double* xinit, double* xout, struct RESULT* results) {
+  set_ok();
+  try {
+    if (B < 1 || M < 1) throw Error(MFISTA_ERR_ARG, "B and M must be >= 1");
+    if (!u_idx || !v_idx || !y_r || !y_i || !noise_stdev || !problems || !xout)
+      throw Error(MFISTA_ERR_ARG, "mfista_fft_batch: null pointer");
+    if (precision != MFISTA_FP64 && precision != MFISTA_FP32)
+      throw Error(MFISTA_ERR_ARG, "the batched FFT variant runs in FP64 or FP32");
+    if (fgp_iter < 1) throw Error(MFISTA_ERR_ARG, "fgp_iter must be >= 1");
+    // epsilon scaled as mfista_imaging_core_fft does (c/mfista_fft_lib.c:715-717)
+    double energy = 0;
+    for (int i = 0; i < M; ++i) energy += y_r[i] * y_r[i] + y_i[i] * y_i[i];
+    const double epsilon = energy * (eps / ((double)M));
+    int form = problems[0].lambda_tv != 0 ? kFormTV : kFormTSV;
+    std::vector<ProbParams> prm(B);
+    for (int b = 0; b < B; ++b) {
+      const mfista_problem& q = problems[b];
+      if (q.lambda_tv != 0 && q.lambda_tsv != 0) throw Error(MFISTA_ERR_BOTH_REG, "lambda_tv and lambda_tsv both non-zero");
+      if ((form == kFormTV) != (q.lambda_tv != 0)) throw Error(MFISTA_ERR_ARG, "mixed TV / TSV problems");
+      if (form == kFormTSV && q.nonneg_flag != 0 && q.nonneg_flag != 1)
+        throw Error(MFISTA_ERR_ARG, "nonneg_flag must be 0 or 1");
+      if (q.maxiter < 0) throw Error(MFISTA_ERR_ARG, "maxiter must be >= 0");
+      prm[b] = ProbParams{q.lambda_l1, q.lambda_tv, q.lambda_tsv, q.cinit, epsilon, q.maxiter, q.nonneg_flag, 0, 0,
+                          q.target_cost};
+    }
+    Solver S;
+    S.precision = precision;
+    S.init_common(B, NX * NY, NX, NY, form, fgp_iter, nullptr);
+    FftVarInput in{u_idx, v_idx, y_r, y_i, noise_stdev, M, NX, NY};
+    if (precision == MFISTA_FP32) S.op.reset(new FftVarOp<float>(S.ctx, in, true));
+    else S.op.reset(new FftVarOp<double>(S.ctx, in));
+    S.finish_setup();
+    double t0 = now_s();
+    S.upload_problems(prm, xinit);
+    S.enqueue_solve(false);
+    std::vector<FinalOut> o;
+    S.fetch(xout, o);
+    double ct = now_s() - t0;
+    int worst = 0;
+    for (int b = 0; b < B; ++b) {
+      if (results) {
+        fill_result(&results[b], o[b], M / 2, (double)M, NX, NY, NX * NY, prm[b].lambda_l1, prm[b].lambda_tv,
+                    prm[b].lambda_tsv, prm[b].maxiter, prm[b].nonneg, ct, false, prm[b].cinit);
+        results[b].residual = nullptr;
+      }
+      if (o[b].status) worst = o[b].status;
+    }
+    if (worst) return fail(worst, "a problem stopped early (status " + std::to_string(worst) + ")", false);
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // operator-level entry points
 // ---------------------------------------------------------------------------
@@ -736,6 +793,62 @@ extern "C" int mfista_fgp_prox(const double* b, int NX, int NY, double lambda_l1
     S.launch_fgp(S.stream);
     MF_CK(cudaMemcpyAsync(x_out, S.ctx.xnew, sizeof(double) * n, cudaMemcpyDeviceToHost, S.stream));
     MF_CK(cudaStreamSynchronize(S.stream));
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
+extern "C" int mfista_fgp_profile(int NX, int NY, int B, int iters, int precision, int reps, double* ms_per_launch,
+                                  double* bytes_per_launch) {
+  set_ok();
+  try {
+    if (NX < 2 || NY < 2 || B < 1 || iters < 1) throw Error(MFISTA_ERR_ARG, "mfista_fgp_profile: bad sizes");
+    const int n = NX * NY;
+    Solver S;
+    S.precision = precision == MFISTA_FP32 ? MFISTA_FP32 : MFISTA_FP64;
+    S.init_common(B, n, NX, NY, kFormTV, iters, nullptr);
+    S.setup_fgp();
+    // every problem a nonnegative FGP prox of a random image at
+    // lambda_tv = 1e-2 (c = 1, dfdx = 0, z = b)
+    std::vector<ProbParams> prm(B);
+    std::vector<ProbState> st(B);
+    std::vector<double> z((size_t)B * n);
+    uint64_t r = 0x2545F4914F6CDD1Dull;
+    for (double& v : z) {
+      r ^= r << 13;
+      r ^= r >> 7;
+      r ^= r << 17;
+      v = (double)(r >> 11) / 9007199254740992.0;
+    }
+    for (int b = 0; b < B; ++b) {
+      memset(&prm[b], 0, sizeof(ProbParams));
+      prm[b].lambda_tv = 1e-2;
+      prm[b].nonneg = 1;
+      memset(&st[b], 0, sizeof(ProbState));
+      st[b].active = 1;
+      st[b].c = 1.0;
+    }
+    MF_CK(cudaMemcpyAsync(S.ctx.prm, prm.data(), sizeof(ProbParams) * B, cudaMemcpyHostToDevice, S.stream));
+    MF_CK(cudaMemcpyAsync(S.ctx.st, st.data(), sizeof(ProbState) * B, cudaMemcpyHostToDevice, S.stream));
+    MF_CK(cudaMemcpyAsync(S.ctx.z, z.data(), sizeof(double) * z.size(), cudaMemcpyHostToDevice, S.stream));
+    MF_CK(cudaMemsetAsync(S.ctx.dfdx, 0, sizeof(double) * z.size(), S.stream));
+    S.launch_fgp(S.stream);  // warm
+    cudaEvent_t e0, e1;
+    MF_CK(cudaEventCreate(&e0));
+    MF_CK(cudaEventCreate(&e1));
+    MF_CK(cudaEventRecord(e0, S.stream));
+    const int R = std::max(1, reps);
+    for (int k = 0; k < R; ++k) S.launch_fgp(S.stream);
+    MF_CK(cudaEventRecord(e1, S.stream));
+    MF_CK(cudaEventSynchronize(e1));
+    float t = 0;
+    MF_CK(cudaEventElapsedTime(&t, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (ms_per_launch) *ms_per_launch = t / R;
+    // compulsory bytes of one prox call: z and dfdx read, xnew written (FP64)
+    if (bytes_per_launch) *bytes_per_launch = 24.0 * (double)B * n;
     return MFISTA_OK;
   } catch (const Error& e) {
     return fail(e.status, e.what(), false);

@@ -604,8 +604,13 @@ template <typename T> struct FftVarOp : Op {
   size_t smem_rows = 0, smem_cols = 0;
   long hstride = 0;
   double sqrtn = 0;
+  // corrected FP32 form: the FP64 operator computes the exact spectrum of
+  // the anchors x_a (d_axa, [B][NX*NYh]); the FP32 transforms then see only
+  // the departure v - x_a
+  std::unique_ptr<FftVarOp<double>> exact;
+  DevMem d_axa;
 
-  FftVarOp(Ctx& ctx, const FftVarInput& in) : c(ctx) {
+  FftVarOp(Ctx& ctx, const FftVarInput& in, bool correct = false) : c(ctx) {
     NX = in.NX;
     NY = in.NY;
     B = ctx.B;
@@ -639,31 +644,68 @@ template <typename T> struct FftVarOp : Op {
     hstride = (long)NX * NYh;
     d_H.alloc(sizeof(cplx<T>) * (size_t)B * hstride);
     sqrtn = sqrt((double)(NX * NY));
-    auto rows_smem = [&](int r) { return (size_t)2 * r * (NY / 2 + 1) * sizeof(cplx<T>); };
-    auto cols_smem = [&](int cc) { return (size_t)2 * cc * (NX + 1) * sizeof(cplx<T>); };
-    while (rpc > 1 && rows_smem(rpc) > 96 * 1024) rpc /= 2;
-    while (cpc > 1 && cols_smem(cpc) > 96 * 1024) cpc /= 2;
-    smem_rows = rows_smem(rpc);
-    smem_cols = cols_smem(cpc);
+    // launch shapes: the FP64 operator's (the larger buffers) bound both, so
+    // that the exact and the FP32 passes write the same partial-sum slots
+    auto fits = [&](int r, int len) { return (size_t)2 * r * (len + 1) * sizeof(cplx<double>) <= 96 * 1024; };
+    while (rpc > 1 && !fits(rpc, NY / 2)) rpc /= 2;
+    while (cpc > 1 && !fits(cpc, NX)) cpc /= 2;
+    set_rpc_cpc(rpc, cpc);
+    if (correct && sizeof(T) == 4) {
+      exact.reset(new FftVarOp<double>(ctx, in, false));
+      exact->set_rpc_cpc(rpc, cpc);
+      d_axa.alloc(sizeof(double2) * (size_t)B * hstride);
+      MF_CK(cudaMemset(d_axa.p, 0, d_axa.bytes));
+    }
+  }
+
+  void set_rpc_cpc(int r, int cc) {
+    rpc = r;
+    cpc = cc;
+    smem_rows = (size_t)2 * rpc * (NY / 2 + 1) * sizeof(cplx<T>);
+    smem_cols = (size_t)2 * cpc * (NX + 1) * sizeof(cplx<T>);
     set_smem(k_fftv_rows_fwd<T>, smem_rows);
     set_smem(k_fftv_rows_inv<T>, smem_rows);
     set_smem(k_fftv_cols<T>, smem_cols);
   }
 
+  void launch_rows_fwd(cudaStream_t s, const double* src, int gate, const double* sub) {
+    k_fftv_rows_fwd<T><<<dim3(cdiv(NX, rpc), B), 256, smem_rows, s>>>(src, c.xstride, d_H.as<cplx<T>>(), hstride, NX,
+                                                                      NY, fh.dev, tw2h.as<cplx<T>>(), c.st, gate, rpc,
+                                                                      sub);
+    MF_LAUNCH_CK();
+  }
+
+  void launch_cols_fwd(cudaStream_t s, int gate, int qchi, bool store, const double2* base, double2* raw_out) {
+    k_fftv_cols<T><<<dim3(cdiv(NYh, cpc), B), 256, smem_cols, s>>>(d_H.as<cplx<T>>(), hstride, NX, NYh, fnx.dev, -1,
+                                                                   cpc, geo, sqrtn, c.st, gate, c.part, qchi,
+                                                                   store ? 1 : 0, base, raw_out);
+    MF_LAUNCH_CK();
+  }
+
   void forward(cudaStream_t s, const double* src, int gate, int qchi, bool store) override {
-    cplx<T>* H = d_H.as<cplx<T>>();
-    k_fftv_rows_fwd<T><<<dim3(cdiv(NX, rpc), B), 256, smem_rows, s>>>(src, c.xstride, H, hstride, NX, NY, fh.dev,
-                                                                      tw2h.as<cplx<T>>(), c.st, gate, rpc);
-    MF_LAUNCH_CK();
-    k_fftv_cols<T><<<dim3(cdiv(NYh, cpc), B), 256, smem_cols, s>>>(H, hstride, NX, NYh, fnx.dev, -1, cpc, geo, sqrtn,
-                                                                   c.st, gate, c.part, qchi, store ? 1 : 0);
-    MF_LAUNCH_CK();
+    // with defect correction: F(v) = F(x_a) (FP64) + F32(v - x_a)
+    launch_rows_fwd(s, src, gate, exact ? c.xa : nullptr);
+    launch_cols_fwd(s, gate, qchi, store, exact ? d_axa.as<double2>() : nullptr, nullptr);
+  }
+
+  bool corrected() const override { return exact != nullptr; }
+  int launches_refresh() const override { return exact ? 2 : 0; }
+
+  void refresh_anchor(cudaStream_t s, int gate) override {
+    if (!exact) return;
+    exact->launch_rows_fwd(s, c.xa, gate, nullptr);
+    exact->launch_cols_fwd(s, gate, -1, false, nullptr, d_axa.as<double2>());
+  }
+
+  void forward_exact(cudaStream_t s, const double* src, int gate, int qchi, bool store) override {
+    if (exact) exact->forward(s, src, gate, qchi, store);
+    else forward(s, src, gate, qchi, store);
   }
 
   void adjoint(cudaStream_t s, const double* z_tsv, int qtsv) override {
     cplx<T>* H = d_H.as<cplx<T>>();
     k_fftv_cols<T><<<dim3(cdiv(NYh, cpc), B), 256, smem_cols, s>>>(H, hstride, NX, NYh, fnx.dev, +1, cpc, geo, sqrtn,
-                                                                   c.st, kGateGrad, c.part, -1, 0);
+                                                                   c.st, kGateGrad, c.part, -1, 0, nullptr, nullptr);
     MF_LAUNCH_CK();
     k_fftv_rows_inv<T><<<dim3(cdiv(NX, rpc), B), 256, smem_rows, s>>>(
         H, hstride, c.dfdx, c.xstride, NX, NY, fh.dev, tw2h.as<cplx<T>>(), z_tsv, c.prm, c.tsvNX, c.tsvNY, c.part,

@@ -150,6 +150,25 @@ def make_c1():
     np.savez_compressed(os.path.join(HERE, "c1_fft.npz"), **out)
 
 
+def make_c1long():
+    """Config 1 run long: the TV form with FGP 50 (the reference built with
+    FGPITER 50) for 1000 iterations with the stopping rule off, and the
+    reference's own spread under a 1e-15 change of one visibility."""
+    g = np.load(os.path.join(HERE, "c1_fft.npz"))
+    args = (g["u_idx"], g["v_idx"], g["y_r"], g["y_i"], g["noise"], 128, 128)
+    lam1, lamtv, cinit = float(g["lam1"]), float(g["lamtv"]), float(g["cinit"])
+    x, res = quiet_call(R.core_fft, *args, 1000, 0.0, lam1, lamtv, 0.0, cinit, nonneg_flag=1, fgp50=True)
+    yr = g["y_r"].copy()
+    yr[0] *= 1 + 1e-15
+    x2, res2 = quiet_call(R.core_fft, g["u_idx"], g["v_idx"], yr, g["y_i"], g["noise"], 128, 128, 1000, 0.0, lam1,
+                          lamtv, 0.0, cinit, nonneg_flag=1, fgp50=True)
+    out = dict(x=x, res=res_arr(res), iters=1000,
+               envelope_x=float(np.linalg.norm(x2 - x) / np.linalg.norm(x)),
+               envelope_cost=abs(res2.finalcost - res.finalcost) / res.finalcost)
+    np.savez_compressed(os.path.join(HERE, "c1_tv50_1000.npz"), **out)
+    print("c1long", res.ITER, res.finalcost, out["envelope_x"], out["envelope_cost"])
+
+
 def make_c2small():
     p = synth.dft_problem(nx=16, n_stations=6, n_hours=10, seed=2, m_vis=150)
     A = np.asarray(p.A)
@@ -168,11 +187,13 @@ def make_c2small():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["c0", "c1", "c2"]
+    which = sys.argv[1:] or ["c0", "c1", "c2", "c1long"]
     if "c0" in which:
         make_c0()
     if "c1" in which:
         make_c1()
     if "c2" in which:
         make_c2small()
+    if "c1long" in which:
+        make_c1long()
     print("golden fixtures written to", HERE)
