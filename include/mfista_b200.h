@@ -324,6 +324,31 @@ int mfista_dft_looe(const double *y, const double *A, int M, int N, int NX, cons
 int mfista_cpp_x2y_nufft(const double *u_dx, const double *v_dy, int M, int Nx, int Ny, const double *xin,
                          double *y_r, double *y_i);
 
+/* Adjoint NUFFT of the reference's C++ build: y2x_nufft
+ * (c++/mfista_nufft_lib.cpp:1151-1219, NUFFT2d1_sngl :189-258, exported by
+ * c++/mfista.hpp:139-140), on the GPU in FP64: the 12-tap spreading with
+ * the Hermitian halo folds done as a deterministic per-cell gather, then the
+ * padded inverse FFT and the C++ grid correction.  xout: [Nx*Ny]. */
+int mfista_cpp_y2x_nufft(const double *u_dx, const double *v_dy, int M, int Nx, int Ny, const double *yin_r,
+                         const double *yin_i, double *xout);
+
+/* The C++ build's solver entry points (c++/mfista_nufft_lib.cpp:1016-1074,
+ * c++/mfista_fft_lib.cpp:425-485) under library-specific names; the C++
+ * build's own names are exported by libmfista_b200_cpp.so
+ * (include/mfista_b200_cpp.h), which forwards here.  NUFFT: the C++
+ * operators above, first-iteration backtracking factor 10, RESULT as its
+ * calc_costs_nufft fills it, the caller's u/v/vis arrays sorted in place,
+ * TSV form only.  FFT: the C library's TSV solve, no TV form. */
+void mfista_cpp_imaging_core_nufft(double *u_dx, double *v_dy, double *vis_r, double *vis_i, double *vis_std,
+                                   int M, int Nx, int Ny, int maxiter, double eps, double lambda_l1,
+                                   double lambda_tv, double lambda_tsv, double cinit, double *xinit, double *xout,
+                                   int nonneg_flag, int box_flag, float *cl_box, struct RESULT *mfista_result);
+void mfista_cpp_imaging_core_fft(int *u_idx, int *v_idx, double *y_r, double *y_i, double *noise_stdev, int M,
+                                 int NX, int NY, int maxiter, double eps, double lambda_l1, double lambda_tv,
+                                 double lambda_tsv, double cinit, double *xinit, double *xout, int nonneg_flag,
+                                 unsigned int fftw_plan_flag, int box_flag, float *cl_box,
+                                 struct RESULT *mfista_result);
+
 /* FGP TV proximal map alone (FGP_L1_box / FGP_nonneg_box,
  * c/mfista_TV_lib.c:189-384) on an NX x NY view: x_out = prox(b). */
 int mfista_fgp_prox(const double *b, int NX, int NY, double lambda_l1, double lambda_tv,

@@ -23,7 +23,7 @@ __all__ = ["RESULT", "Problem", "MfistaError", "lib", "mfista_imaging_core_nufft
            "mfista_imaging_core_fft", "mfista_imaging_core_dft", "imaging_core_nufft",
            "imaging_core_fft", "imaging_core_dft", "nufft_batch", "fft_batch", "fgp_profile", "dft_batch", "Plan", "nufft_forward",
            "nufft_adjoint", "fgp_prox", "nufft_lipschitz", "last_status", "last_error", "set_fgp_iter", "set_device",
-           "dft_apply", "dft_profile", "FP64", "FP32", "BF16X3", "BF16X6"]
+           "dft_apply", "dft_profile", "cpp_x2y_nufft", "cpp_y2x_nufft", "cpp_imaging_core_nufft", "FP64", "FP32", "BF16X3", "BF16X6"]
 
 FP64 = 64
 FP32 = 32
@@ -141,6 +141,12 @@ def lib():
         L.mfista_nufft_movie.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, C.c_int, C.c_int, C.c_int, _dp, C.c_double,
                                          C.c_double, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int, _dp,
                                          _dp, C.POINTER(RESULT), _dp]
+        L.mfista_cpp_y2x_nufft.restype = C.c_int
+        L.mfista_cpp_y2x_nufft.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]
+        L.mfista_cpp_imaging_core_nufft.restype = None
+        L.mfista_cpp_imaging_core_nufft.argtypes = L.mfista_imaging_core_nufft.argtypes
+        L.mfista_cpp_imaging_core_fft.restype = None
+        L.mfista_cpp_imaging_core_fft.argtypes = L.mfista_imaging_core_fft.argtypes
         L.mfista_cpp_x2y_nufft.restype = C.c_int
         L.mfista_cpp_x2y_nufft.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]
         L.mfista_dft_looe.restype = C.c_int
@@ -427,6 +433,33 @@ def cpp_x2y_nufft(u_dx, v_dy, nx, ny, x):
     yr, yi = np.zeros(u.size), np.zeros(u.size)
     _check(lib().mfista_cpp_x2y_nufft(_p(u), _p(v), u.size, nx, ny, _p(xx), _p(yr), _p(yi)))
     return yr, yi
+
+
+def cpp_y2x_nufft(u_dx, v_dy, nx, ny, y_r, y_i):
+    """Adjoint NUFFT of the reference's C++ build (y2x_nufft) on the GPU."""
+    u, v, yr, yi = (_d(a) for a in (u_dx, v_dy, y_r, y_i))
+    x = np.zeros(nx * ny)
+    _check(lib().mfista_cpp_y2x_nufft(_p(u), _p(v), u.size, nx, ny, _p(yr), _p(yi), _p(x)))
+    return x
+
+
+def cpp_imaging_core_nufft(u_dx, v_dy, vis_r, vis_i, vis_std, nx, ny, maxiter, eps, lambda_l1, lambda_tv,
+                           lambda_tsv, cinit, xinit=None, nonneg_flag=1, box_flag=0, cl_box=None, xout=None):
+    """The C++ build's mfista_imaging_core_nufft.  Like it, the call sorts
+    the five point arrays in place: pass float64 contiguous arrays to see
+    the permutation (other inputs are converted, and the copies sorted)."""
+    u, v, vr, vi, vs = (a if isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous
+                        else _d(a) for a in (u_dx, v_dy, vis_r, vis_i, vis_std))
+    n = nx * ny
+    xi = np.zeros(n) if xinit is None else _d(xinit)
+    xo = np.zeros(n) if xout is None else np.array(xout, np.float64, copy=True)
+    box = _box(n, cl_box)
+    res = RESULT()
+    lib().mfista_cpp_imaging_core_nufft(_p(u), _p(v), _p(vr), _p(vi), _p(vs), u.size, nx, ny, maxiter, eps,
+                                        lambda_l1, lambda_tv, lambda_tsv, cinit, _p(xi), _p(xo), nonneg_flag,
+                                        box_flag, _p(box, _fp), C.byref(res))
+    _check()
+    return xo, res.as_dict()
 
 
 def dft_looe(y, A, X, nx, lambda_tsv=None):

@@ -983,3 +983,174 @@ extern "C" int mfista_cpp_x2y_nufft(const double* u_dx, const double* v_dy, int 
     return fail(e.status, e.what(), false);
   }
 }
+
+// ---------------------------------------------------------------------------
+// the reference's C++ build (c++/mfista_nufft_lib.cpp, c++/mfista_fft_lib.cpp)
+// ---------------------------------------------------------------------------
+namespace {
+
+// sort_input (c++/mfista_nufft_lib.cpp:550-641): the points ordered by their
+// rounded grid row of v, then of u, with std::sort and the reference's
+// comparator; the five arrays are permuted in place.
+void cpp_sort_input(int M, int Nx, int Ny, double* u, double* v, double* vr, double* vi, double* vs) {
+  const int mrx = 2 * Nx, mry = 2 * Ny;
+  std::vector<size_t> idx(M);
+  for (int i = 0; i < M; ++i) idx[i] = (size_t)i;
+  std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) {
+    const double va = round(v[a] * mry / (2 * M_PI)), vb = round(v[b] * mry / (2 * M_PI));
+    if (va == vb) return round(u[a] * mrx / (2 * M_PI)) < round(u[b] * mrx / (2 * M_PI));
+    return va < vb;
+  });
+  std::vector<double> tmp(M);
+  for (double* arr : {u, v, vr, vi, vs}) {
+    for (int i = 0; i < M; ++i) tmp[i] = arr[i];
+    for (int i = 0; i < M; ++i) arr[i] = tmp[idx[i]];
+  }
+}
+
+// calc_costs_nufft (c++/mfista_nufft_lib.cpp:931-998): the fields it sets
+void fill_costs_cpp(RESULT* r, const FinalOut& o, int M, int nx, int ny, double l1, double ltv, double ltsv) {
+  r->sq_error = o.sq_error;
+  r->M = M;
+  r->N = nx * ny;
+  r->NX = nx;
+  r->NY = ny;
+  r->lambda_l1 = l1;
+  r->lambda_tv = ltv;
+  r->lambda_tsv = ltsv;
+  r->mean_sq_error = o.sq_error / (double)M;
+  r->l1cost = o.l1cost;
+  r->N_active = (int)llround(o.n_active);
+  double fc = o.sq_error / 2;
+  if (l1 > 0) fc += l1 * o.l1cost;
+  if (ltsv > 0) {
+    r->tsvcost = o.regcost;
+    fc += ltsv * o.regcost;
+  }
+  r->finalcost = fc;
+}
+
+// summary (costs) of the C++-build NUFFT problem at x0, no iterations
+void cpp_costs_at(const double* u, const double* v, const double* vr, const double* vi, const double* vs, int M,
+                  int Nx, int Ny, const ProbParams& p, const double* x0, FinalOut& out) {
+  Solver S;
+  S.precision = MFISTA_FP64;
+  S.init_common(1, Nx * Ny, Nx, Ny, kFormTSV, 100, nullptr);
+  S.op.reset(new cppnufft::CppNufftOp(S.ctx, u, v, vr, vi, vs, M, Nx, Ny));
+  S.finish_setup();
+  S.upload_problems({p}, x0);
+  S.enqueue_solve(true);
+  std::vector<FinalOut> o;
+  S.fetch(nullptr, o);
+  out = o[0];
+}
+
+}  // namespace
+
+extern "C" int mfista_cpp_y2x_nufft(const double* u_dx, const double* v_dy, int M, int Nx, int Ny,
+                                    const double* yin_r, const double* yin_i, double* xout) {
+  set_ok();
+  try {
+    if (M < 1 || Nx < 12 || Ny < 12) throw Error(MFISTA_ERR_ARG, "mfista_cpp_y2x_nufft: needs M >= 1, Nx, Ny >= 12");
+    if (!u_dx || !v_dy || !yin_r || !yin_i || !xout) throw Error(MFISTA_ERR_ARG, "mfista_cpp_y2x_nufft: null pointer");
+    Solver S;
+    S.precision = MFISTA_FP64;
+    S.init_common(1, Nx * Ny, Nx, Ny, kFormTSV, 100, nullptr);
+    std::vector<double> zero(M, 0.0), one(M, 1.0);
+    cppnufft::CppNufftOp* op = new cppnufft::CppNufftOp(S.ctx, u_dx, v_dy, zero.data(), zero.data(), one.data(), M,
+                                                        Nx, Ny);
+    S.op.reset(op);
+    std::vector<double2> y(M);
+    for (int k = 0; k < M; ++k) y[k] = make_double2(yin_r[k], yin_i[k]);
+    MF_CK(cudaMemcpyAsync(op->y2(), y.data(), sizeof(double2) * (size_t)M, cudaMemcpyHostToDevice, S.stream));
+    ProbState st;
+    memset(&st, 0, sizeof(st));
+    st.active = 1;
+    MF_CK(cudaMemcpyAsync(S.ctx.st, &st, sizeof(st), cudaMemcpyHostToDevice, S.stream));
+    op->adjoint_into(S.stream, S.ctx.dfdx, nullptr, -1, kGateAll);
+    MF_CK(cudaMemcpyAsync(xout, S.ctx.dfdx, sizeof(double) * (size_t)Nx * Ny, cudaMemcpyDeviceToHost, S.stream));
+    MF_CK(cudaStreamSynchronize(S.stream));
+    return MFISTA_OK;
+  } catch (const Error& e) {
+    return fail(e.status, e.what(), false);
+  }
+}
+
+// mfista_imaging_core_nufft of the C++ build (c++/mfista_nufft_lib.cpp:1016-1074):
+// RESULT from calc_costs_nufft (M = M, not M/2), TSV form only, the caller's
+// u/v/vis arrays sorted in place, first-iteration backtracking factor 10.
+extern "C" void mfista_cpp_imaging_core_nufft(double* u_dx, double* v_dy, double* vis_r, double* vis_i,
+                                              double* vis_std, int M, int Nx, int Ny, int maxiter, double eps,
+                                              double lambda_l1, double lambda_tv, double lambda_tsv, double cinit,
+                                              double* xinit, double* xout, int nonneg_flag, int box_flag,
+                                              float* cl_box, struct RESULT* mfista_costs) {
+  set_ok();
+  try {
+    if (maxiter < 0) throw Error(MFISTA_ERR_ARG, "maxiter must be >= 0");
+    double epsilon = 0;
+    for (int i = 0; i < M; ++i) epsilon += vis_r[i] * vis_r[i] + vis_i[i] * vis_i[i];
+    epsilon *= eps / ((double)M);
+    const int N = Nx * Ny;
+    // costs at xinit (:1037-1040)
+    ProbParams p0{lambda_l1, 0.0, lambda_tsv, cinit, epsilon, 0, 1, 0, 0, 0.0};
+    FinalOut o;
+    cpp_costs_at(u_dx, v_dy, vis_r, vis_i, vis_std, M, Nx, Ny, p0, xinit, o);
+    fill_costs_cpp(mfista_costs, o, M, Nx, Ny, lambda_l1, lambda_tv, lambda_tsv);
+    if (lambda_tv != 0) {
+      printf("We have not implemented TV option.\n");
+      fail(MFISTA_ERR_ARG, "the C++ build has no TV form", false);
+      return;
+    }
+    cpp_sort_input(M, Nx, Ny, u_dx, v_dy, vis_r, vis_i, vis_std);
+    double t0 = now_s();
+    if (nonneg_flag != 0 && nonneg_flag != 1) {
+      // the C++ core returns 0 iterations without writing xout (:789-795)
+      printf("nonneg_flag must be chosen properly.\n");
+      cpp_costs_at(u_dx, v_dy, vis_r, vis_i, vis_std, M, Nx, Ny, p0, xout, o);
+      mfista_costs->comp_time = now_s() - t0;
+      mfista_costs->ITER = 0;
+      mfista_costs->Lip_const = cinit;
+    } else {
+      ProbParams p{lambda_l1, 0.0, lambda_tsv, cinit, epsilon, maxiter, nonneg_flag, box_flag, 0, 0.0};
+      Solver S;
+      S.precision = MFISTA_FP64;
+      S.eta_first = 10.0;
+      S.init_common(1, N, Nx, Ny, kFormTSV, 100, box_flag == 1 ? cl_box : nullptr);
+      S.op.reset(new cppnufft::CppNufftOp(S.ctx, u_dx, v_dy, vis_r, vis_i, vis_std, M, Nx, Ny));
+      S.finish_setup();
+      t0 = now_s();
+      S.upload_problems({p}, xinit);
+      S.enqueue_solve(maxiter == 0);
+      std::vector<FinalOut> oo;
+      S.fetch(xout, oo);
+      o = oo[0];
+      mfista_costs->comp_time = now_s() - t0;
+      mfista_costs->ITER = o.iters;
+      mfista_costs->Lip_const = maxiter == 0 ? cinit : o.lip;
+      if (o.status) fail(o.status, "solver stopped early (status " + std::to_string(o.status) + ")", !quiet());
+    }
+    mfista_costs->nonneg = nonneg_flag;
+    mfista_costs->maxiter = maxiter;
+    fill_costs_cpp(mfista_costs, o, M, Nx, Ny, lambda_l1, lambda_tv, lambda_tsv);
+  } catch (const Error& e) {
+    fail(e.status, e.what(), true);
+  }
+}
+
+// mfista_imaging_core_fft of the C++ build (c++/mfista_fft_lib.cpp:425-485):
+// the C library's TSV solve; the TV form is not implemented there.
+extern "C" void mfista_cpp_imaging_core_fft(int* u_idx, int* v_idx, double* y_r, double* y_i, double* noise_stdev,
+                                            int M, int NX, int NY, int maxiter, double eps, double lambda_l1,
+                                            double lambda_tv, double lambda_tsv, double cinit, double* xinit,
+                                            double* xout, int nonneg_flag, unsigned int fftw_plan_flag, int box_flag,
+                                            float* cl_box, struct RESULT* mfista_result) {
+  if (lambda_tv != 0) {
+    set_ok();
+    printf("We have not implemented TV option.\n");
+    fail(MFISTA_ERR_ARG, "the C++ build has no TV form", false);
+    return;
+  }
+  mfista_imaging_core_fft(u_idx, v_idx, y_r, y_i, noise_stdev, M, NX, NY, maxiter, eps, lambda_l1, lambda_tv,
+                          lambda_tsv, cinit, xinit, xout, nonneg_flag, fftw_plan_flag, box_flag, cl_box,
+                          mfista_result);
+}

@@ -268,6 +268,10 @@ struct CtrlCfg {
   int joint;
   double lam_t;
   double* jq;
+  // > 0: backtracking factor of the first outer iteration (the reference's
+  // C++ build starts with 10, c++/mfista_nufft_lib.cpp:818, :860-863);
+  // 0: ETA throughout (the C library)
+  double eta_first;
 };
 
 // status codes written to ProbState.status (values of enum mfista_status)
@@ -468,7 +472,7 @@ __global__ void __launch_bounds__(128) k_control(const ProbParams* __restrict__ 
       } else {
         bool finish = fval <= qval + cfg.bt_slack * fabs(qval);
         if (!finish) {
-          s.c *= kEta;
+          s.c *= (s.iter == 0 && cfg.eta_first > 0) ? cfg.eta_first : kEta;
           s.trial += 1;
           finish = s.trial >= p.maxiter;  // backtracking loop exhausted
         }

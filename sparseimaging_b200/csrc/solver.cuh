@@ -1071,6 +1071,8 @@ struct Solver {
   bool joint = false;
   double lam_t = 0.0;
   DevMem d_wt, d_jq;
+  // first-iteration backtracking factor (0: ETA, the C library's loop)
+  double eta_first = 0.0;
 
   void set_movie(const std::vector<double>& wt, double lam) {
     joint = true;
@@ -1289,6 +1291,7 @@ struct Solver {
     cfg.jq = d_jq.as<double>();
     cfg.slots[kQDtZ] = joint ? img_blocks() : 0;
     cfg.slots[kQDtX] = joint ? img_blocks() : 0;
+    cfg.eta_first = eta_first;
     return cfg;
   }
 

@@ -121,3 +121,20 @@ int main(int argc, char **argv) { if (argc > 99) x2y_nufft(0, 0, 0, 0, 0, 0, 0, 
     libdir = os.path.dirname(build.LIB)
     subprocess.run(["gcc", "-Werror", "-o", str(tmp_path / "shim"), str(src), f"-L{libdir}",
                     f"-l:{os.path.basename(build.LIB)}", f"-Wl,-rpath,{libdir}"], check=True)
+
+
+def test_cpp_build_library_exports_the_cpp_names():
+    """libmfista_b200_cpp.so exports the names of the reference's C++ build
+    (c++/mfista.hpp:115-140) declared in include/mfista_b200_cpp.h."""
+    from sparseimaging_b200 import build
+    build.build(verbose=False)
+    hdr = open(os.path.join(ROOT, "include", "mfista_b200_cpp.h")).read()
+    hdr = re.sub(r"/\*.*?\*/", "", hdr, flags=re.S)
+    names = sorted(set(re.findall(r"\b(\w+)\s*\(", hdr)))
+    assert names == ["mfista_imaging_core_fft", "mfista_imaging_core_nufft", "x2y_nufft", "y2x_nufft"]
+    out = subprocess.run(["nm", "-D", "--defined-only", build.CPP_LIB], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (\w+)", out))
+    assert set(names) <= exported
+    lib = C.CDLL(build.CPP_LIB)
+    for n in names:
+        assert hasattr(lib, n)
