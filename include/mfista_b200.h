@@ -276,12 +276,19 @@ int mfista_nufft_adjoint(const double *u_dx, const double *v_dy, int M, int Nx, 
  * All intermediates live in one fixed device array of
  * MFISTA_NOALLOC_SCRATCH_BYTES, which a device holds from the first call on
  * it (earlier where CUDA loads modules eagerly) until the process exits;
- * nothing is allocated or freed.  Inputs whose working set (about 32*Nx*(Ny+1) + 8*Nx*Ny + 408*M bytes) exceeds it, and
- * Nx > 767 or Ny > 1535, are rejected with MFISTA_ERR_ARG.  The first call
- * on a device looks up the array's address there: make it before any stream
- * capture.  Calls share the array, so calls that may run at the same time on
- * one GPU race and must be ordered by the caller.  Returns an mfista_status;
- * mfista_last_status/error are not updated. */
+ * nothing is allocated or freed.  Inputs whose working set exceeds it, and
+ * Nx > 767 or Ny > 1535, are rejected with MFISTA_ERR_ARG.  The working set
+ * is approximately 32*Nx*(Ny+1) + 8*Nx*Ny + 408*M bytes (each of its 13
+ * pieces is rounded up to 256 bytes and the FFT twiddle tables add
+ * 16*(3*Ny + 2*Nx) bytes), so inputs near the limit may be rejected.  The
+ * first call on a device looks up the array's address there and keeps it:
+ * make it before any stream capture, and do not call this entry point on a
+ * device after a cudaDeviceReset of it (the kept address is then stale).  A
+ * CUDA error already pending in the calling thread is reported as
+ * MFISTA_ERR_CUDA and left pending.  Calls share the array, so calls that
+ * may run at the same time on one GPU race and must be ordered by the
+ * caller.  Returns an mfista_status; mfista_last_status/error are not
+ * updated. */
 #define MFISTA_NOALLOC_SCRATCH_BYTES (16u << 20)
 int mfista_nufft_forward_noalloc(const double *u_dx, const double *v_dy, int M, int Nx, int Ny,
                                  const double *x, double *out_r, double *out_i, void *stream);

@@ -20,8 +20,15 @@
 //   * inputs whose working set does not fit it are rejected with
 //     MFISTA_ERR_ARG before any work is enqueued;
 //   * the first call on a device looks up the array's device address there
-//     (cudaGetSymbolAddress, with that device current): make that first call
-//     before any stream capture;
+//     (cudaGetSymbolAddress, with that device current) and keeps it: make
+//     that first call before any stream capture.  A cudaDeviceReset unloads
+//     the array with the rest of the device's state, and the kept address
+//     then points at freed memory: after resetting a device, do not call this
+//     entry point on it again in the same process;
+//   * a CUDA error already pending in the calling thread when the call starts
+//     (an earlier launch of the caller's that failed) is reported as
+//     MFISTA_ERR_CUDA before anything is enqueued, and left pending for the
+//     caller to read;
 //   * every call uses the same array and leaves its contents behind; calls
 //     that run at the same time on one GPU (two streams, two host threads)
 //     race on it and must be ordered by the caller;
@@ -147,6 +154,8 @@ extern "C" int mfista_nufft_forward_noalloc(const double* u_dx, const double* v_
   const size_t o_lo = cv.take<int>(1);
   const size_t o_hi = cv.take<int>(1);
   if (cv.off > kNoAllocBytes) return MFISTA_ERR_ARG;
+  // an error pending from the caller's own work: report it, do not consume it
+  if (cudaPeekAtLastError() != cudaSuccess) return MFISTA_ERR_CUDA;
   FftDev<double> fh, fcol;
   if (!factor(Ny, fh) || !factor(2 * Nx, fcol)) return MFISTA_ERR_ARG;
   // one row / one column per CTA, ping-pong buffers in shared memory
@@ -164,7 +173,7 @@ extern "C" int mfista_nufft_forward_noalloc(const double* u_dx, const double* v_
       void* p = nullptr;
       cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess || !p) {
-        cudaGetLastError();
+        cudaGetLastError();  // this call's own error (none was pending on entry)
         return MFISTA_ERR_CUDA;
       }
       g_scratch_dev[dev] = static_cast<unsigned char*>(p);
@@ -226,5 +235,6 @@ extern "C" int mfista_nufft_forward_noalloc(const double* u_dx, const double* v_
       geo, grid, 0, Nx, Ny, 1.0 / ((double)(2 * Nx) * (double)(2 * Ny)), st, kGateAll, none, -1, nullptr, 1, nullptr,
       ax, ppw);
   k_noalloc_split<<<cdiv_i(M, T), T, 0, s>>>(ax, M, out_r, out_i);
+  // nothing was pending on entry, so an error now is one of these launches
   return cudaGetLastError() == cudaSuccess ? MFISTA_OK : MFISTA_ERR_CUDA;
 }

@@ -62,6 +62,28 @@ def test_noalloc_forward_matches_allocating_entry_point(gpulib, c0):
     assert rel(outs[0][0] + 1j * outs[0][1], c0["fwd_r"] + 1j * c0["fwd_i"]) < 1e-12
 
 
+def test_noalloc_forward_takes_no_device_memory(gpulib, c0):
+    """Once a device has the scratch array, a call leaves the device's free
+    memory unchanged (cudaMemGetInfo before and after)."""
+    import torch
+    f = _noalloc(gpulib)
+    dev = torch.device("cuda:0")
+    u2, v2, x2 = _case_128()
+    bufs = [torch.from_numpy(np.ascontiguousarray(a, np.float64)).to(dev) for a in (u2, v2, x2)]
+    o_r = torch.zeros(u2.size, dtype=torch.float64, device=dev)
+    o_i = torch.zeros(u2.size, dtype=torch.float64, device=dev)
+    args = (bufs[0].data_ptr(), bufs[1].data_ptr(), u2.size, 128, 128, bufs[2].data_ptr(), o_r.data_ptr(),
+            o_i.data_ptr(), None)
+    assert f(*args) == 0  # the device has its array and kernels from here on
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    assert f(*args) == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(dev)[0] == free0
+    fr, fi = gpulib.nufft_forward(u2, v2, 128, 128, x2)
+    assert rel(o_r.cpu().numpy() + 1j * o_i.cpu().numpy(), fr + 1j * fi) < 1e-12
+
+
 def test_noalloc_forward_rejects_sizes_beyond_its_scratch(gpulib):
     import torch
     f = _noalloc(gpulib)
