@@ -170,11 +170,34 @@ __global__ void k_stats(const double* __restrict__ vall, const double* __restric
 //   monotone improvement: z = x (1-mu)/mu' + xnew (1 + (mu-1)/mu'); x = xnew
 //   otherwise:            z = x (1 - mu/mu') + xnew mu/mu'
 // ---------------------------------------------------------------------------
+// Kept visibility models of the corrected FP32 NUFFT form, updated with the
+// same momentum (az = mom_a ax + mom_b axn, ax = axn when the trial point is
+// taken) by the CTAs of k_momentum beyond the image's: one launch for both.
+struct ModelMom {
+  const int* pt_lo;
+  const int* pt_hi;
+  long bstride;
+  double2* ax;
+  const double2* axn;
+  double2* az;
+  int img_blocks;  // CTAs of the image part; the rest cover points
+};
+
 __global__ void k_momentum(double* __restrict__ xall, double* __restrict__ zall, const double* __restrict__ xnall,
-                           ImgDims dm, const ProbState* __restrict__ st) {
+                           ImgDims dm, const ProbState* __restrict__ st, ModelMom mm) {
   int b = blockIdx.y;
   const ProbState& s = st[b];
   if (!s.accepted) return;
+  if (mm.ax && (int)blockIdx.x >= mm.img_blocks) {
+    const int k = mm.pt_lo[b] + ((int)blockIdx.x - mm.img_blocks) * blockDim.x + threadIdx.x;
+    if (k >= mm.pt_hi[b]) return;
+    const size_t e = (size_t)b * mm.bstride + k;
+    const double2 x = mm.ax[e], xn = mm.axn[e];
+    mm.az[e] = make_double2(s.mom_a * x.x + s.mom_b * xn.x, s.mom_a * x.y + s.mom_b * xn.y);
+    if (s.take_x) mm.ax[e] = xn;
+    return;
+  }
+  if ((int)blockIdx.x >= mm.img_blocks) return;
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= dm.N) return;
   double* x = xall + (size_t)b * dm.xstride;

@@ -1052,22 +1052,6 @@ __global__ void k_nufft_resid_model(NufftGeom<T> geo, const double2* __restrict_
   }
 }
 
-// after the control step: az = mom_a ax + mom_b axn and ax = axn when the
-// trial point was taken (problems whose step was accepted)
-static __global__ void k_nufft_model_momentum(const int* __restrict__ pt_lo, const int* __restrict__ pt_hi, long bstride,
-                                       double2* __restrict__ ax, const double2* __restrict__ axn,
-                                       double2* __restrict__ az, const ProbState* __restrict__ st) {
-  const int b = blockIdx.y;
-  const ProbState& s = st[b];
-  if (!s.accepted) return;
-  const int k = pt_lo[b] + blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= pt_hi[b]) return;
-  const size_t e = (size_t)b * bstride + k;
-  const double2 x = ax[e], xn = axn[e];
-  az[e] = make_double2(s.mom_a * x.x + s.mom_b * xn.x, s.mom_a * x.y + s.mom_b * xn.y);
-  if (s.take_x) ax[e] = xn;
-}
-
 // ax = src (and az = src when az is given) for the problems passing `gate`
 static __global__ void k_nufft_model_set(const int* __restrict__ pt_lo, const int* __restrict__ pt_hi, long bstride,
                                   const double2* __restrict__ src, double2* __restrict__ ax,

@@ -183,11 +183,17 @@ struct Op {
   virtual int refresh_period() const { return 32; }
   // forward model at the momentum point z by linearity from kept models of
   // x and of the trial point (operators that keep them return true):
-  // forward_z replaces forward(z, ...) (residual kept, chi^2 into qchi),
-  // model_momentum follows k_momentum
+  // forward_z replaces forward(z, ...) (residual kept, chi^2 into qchi);
+  // model_momentum gives k_momentum the models to update with the images
   virtual bool models_z() const { return false; }
   virtual void forward_z(cudaStream_t s, int gate, int qchi) { (void)s; (void)gate; (void)qchi; }
-  virtual void model_momentum(cudaStream_t s) { (void)s; }
+  virtual ModelMom model_momentum(int img_blocks) {
+    ModelMom m;
+    memset(&m, 0, sizeof(m));
+    m.img_blocks = img_blocks;
+    return m;
+  }
+  virtual int model_blocks() const { return 0; }
 };
 
 // ---------------------------------------------------------------------------
@@ -433,12 +439,18 @@ template <typename T> struct NufftOp : Op {
     MF_LAUNCH_CK();
   }
 
-  void model_momentum(cudaStream_t s) override {
-    if (!model) return;
-    k_nufft_model_momentum<<<dim3(std::max(1, cdiv(mmax, 256)), B), 256, 0, s>>>(
-        geo.pt_lo, geo.pt_hi, geo.y2_bstride, d_ax.as<double2>(), d_axn.as<double2>(), d_az.as<double2>(), c.st);
-    MF_LAUNCH_CK();
+  ModelMom model_momentum(int img_blocks) override {
+    ModelMom m = Op::model_momentum(img_blocks);
+    if (!model) return m;
+    m.pt_lo = geo.pt_lo;
+    m.pt_hi = geo.pt_hi;
+    m.bstride = geo.y2_bstride;
+    m.ax = d_ax.as<double2>();
+    m.axn = d_axn.as<double2>();
+    m.az = d_az.as<double2>();
+    return m;
   }
+  int model_blocks() const override { return model ? std::max(1, cdiv(mmax, 256)) : 0; }
 
   void forward_exact(cudaStream_t s, const double* src, int gate, int qchi, bool store) override {
     if (exact) exact->forward(s, src, gate, qchi, store);
@@ -1158,7 +1170,7 @@ struct Solver {
     // and the rest (trial point, its forward pass, control, momentum)
     ref_block_launches = op->corrected() ? 1 + op->launches_refresh() : 0;
     grad_block_launches = (op->models_z() ? 1 : op->launches_forward()) + op->launches_adjoint() + (joint ? 1 : 0);
-    rest_launches = op->launches_forward() + 3 + (form == kFormTV ? 1 : 0) + (op->models_z() ? 1 : 0) + (joint ? 1 : 0);
+    rest_launches = op->launches_forward() + 3 + (form == kFormTV ? 1 : 0) + (joint ? 1 : 0);
     per_step_launches = ref_block_launches + grad_block_launches + rest_launches;
     fixed_launches = 2 * (op->launches_forward() + 2) + 1 + (joint ? 2 : 0);
     const char* hl = getenv("MFISTA_HOST_LOOP");
@@ -1376,9 +1388,11 @@ struct Solver {
     }
     op->forward(s, ctx.xnew, kGateTrial, kQChiX, false);
     launch_control(s, kCtrlStep, h, set_handle);
-    k_momentum<<<ig, 256, 0, s>>>(ctx.x, ctx.z, ctx.xnew, dm, ctx.st);
+    // image momentum and, for operators that keep visibility models, the
+    // models' momentum in the same launch
+    k_momentum<<<dim3(img_blocks() + op->model_blocks(), ctx.B), 256, 0, s>>>(ctx.x, ctx.z, ctx.xnew, dm, ctx.st,
+                                                                            op->model_momentum(img_blocks()));
     MF_LAUNCH_CK();
-    op->model_momentum(s);
   }
 
   void drop_graphs() {
