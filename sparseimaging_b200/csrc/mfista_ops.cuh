@@ -311,7 +311,9 @@ struct FinalOut {       // one per problem, read back by the host
 };
 
 __device__ __forceinline__ double warp_partial_sum(const double* p, int n, int lane) {
+  // loads issued 8 ahead (the partials are independent), sums in slot order
   double s = 0.0;
+#pragma unroll 8
   for (int i = lane; i < n; i += 32) s += p[i];
   return warp_sum(s);
 }
@@ -423,10 +425,12 @@ __device__ void control_joint(const ProbParams* __restrict__ prm, ProbState* __r
   *ticket = 0u;
 }
 
-// One CTA per problem.  The four warps reduce the partial sums (fixed order),
+// One CTA per problem.  One warp per quantity reduces its partial sums (fixed order),
 // thread 0 runs the MFISTA scalar logic, and the last CTA to finish (atomic
 // ticket) ORs the active flags into the graph's WHILE condition.
-__global__ void __launch_bounds__(128) k_control(const ProbParams* __restrict__ prm, ProbState* __restrict__ st,
+constexpr int kControlThreads = 32 * kNumQ;  // one warp per reduced quantity
+
+__global__ void __launch_bounds__(kControlThreads) k_control(const ProbParams* __restrict__ prm, ProbState* __restrict__ st,
                                                  Partials part, CtrlCfg cfg, FinalOut* __restrict__ out,
                                                  cudaGraphConditionalHandle handle, int set_handle,
                                                  int* __restrict__ any_active, unsigned int* __restrict__ ticket) {
@@ -437,7 +441,7 @@ __global__ void __launch_bounds__(128) k_control(const ProbParams* __restrict__ 
   if (threadIdx.x == 0) s_skip = (cfg.mode == kCtrlStep && !st[b].active) ? 1 : 0;
   __syncthreads();
   if (!s_skip) {
-    for (int q = warp; q < kNumQ; q += 4) {
+    for (int q = warp; q < kNumQ; q += kControlThreads / 32) {
       bool need = q == kQChiX || q == kQL1 || q == kQReg;
       if (cfg.mode == kCtrlStep) need = need || q == kQChiZ || q == kQTsvZ || q == kQDq1 || q == kQDq2;
       if (cfg.mode == kCtrlFinal) need = need || q == kQNact;

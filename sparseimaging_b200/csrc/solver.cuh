@@ -1308,7 +1308,7 @@ struct Solver {
   }
 
   void launch_control(cudaStream_t s, int mode, cudaGraphConditionalHandle h, int set_handle) {
-    k_control<<<ctx.B, 128, 0, s>>>(ctx.prm, ctx.st, ctx.part, ctrl_cfg(mode), d_out.as<FinalOut>(), h, set_handle,
+    k_control<<<ctx.B, kControlThreads, 0, s>>>(ctx.prm, ctx.st, ctx.part, ctrl_cfg(mode), d_out.as<FinalOut>(), h, set_handle,
                                      d_any, d_ticket.as<unsigned int>());
     MF_LAUNCH_CK();
   }
