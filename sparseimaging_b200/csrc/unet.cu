@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -160,6 +161,131 @@ __global__ void __launch_bounds__(128) k_conv3x3(ConvArgs g) {
     }
   }
 }
+
+// ---------------------------------------------------------------------------
+// The same 3x3 convolution as an implicit GEMM on the tensor cores
+// (mma.sync m16n8k16, BF16 operands, FP32 accumulation):
+//   out[co][pix] = sum_{tap, ci} W[co][ci][tap] X[ci][pix + tap]
+// with K ordered tap-major (one k16 step = one tap x 16 input channels).
+// The weights are BF16 already; an FP32 activation x enters as the two BF16
+// planes hi = bf16(x), lo = bf16(x - hi), whose sum is x to 2^-18 relative,
+// so every product is W hi + W lo, two MMAs, accumulated in FP32.
+// Block: a 16 x 16 output tile and 16 * MT output channels, 8 warps; warp w
+// owns output rows 2w, 2w + 1 (four n8 tiles of 8 pixels).  Per chunk of 16
+// input channels the halo tile (18 x 18 pixels, channel-minor, both planes)
+// and the chunk's weights ([tap][co][ci]) are staged in shared memory with
+// 24 BF16 per row, which makes the fragment loads bank-conflict free.
+// Deterministic: the MMA sequence is fixed.
+// ---------------------------------------------------------------------------
+constexpr int kTcRow = 12;                       // 32-bit words per staged pixel / weight row (16 used)
+constexpr int kTcHalo = (kCT + 2) * (kCT + 2);   // 324 halo pixels
+
+__device__ __forceinline__ void mma_bf16_16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+template <int MT>
+__global__ void __launch_bounds__(256) k_conv3x3_tc(ConvArgs g) {
+  constexpr int CO = 16 * MT;
+  extern __shared__ __align__(16) uint32_t s_tc[];
+  uint32_t* s_x = s_tc;                                  // [2][324][kTcRow]
+  uint32_t* s_w = s_tc + 2 * kTcHalo * kTcRow;           // [9][CO][kTcRow]
+  __nv_bfloat16* s_x16 = reinterpret_cast<__nv_bfloat16*>(s_x);
+  __nv_bfloat16* s_w16 = reinterpret_cast<__nv_bfloat16*>(s_w);
+  const int tiles_x = cdiv(g.W, kCT);
+  const int tx0 = (blockIdx.x % tiles_x) * kCT, ty0 = (blockIdx.x / tiles_x) * kCT;
+  const int co0 = blockIdx.y * CO, n = blockIdx.z;
+  const int cin = g.ca + g.cb;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gid = lane >> 2, tig = lane & 3;
+  float acc[MT][4][4];
+#pragma unroll
+  for (int m = 0; m < MT; ++m)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[m][j][e] = 0.f;
+  const int ha = g.a_up ? g.H / 2 : g.H, wa = g.a_up ? g.W / 2 : g.W;
+  for (int c0 = 0; c0 < cin; c0 += kCI) {
+    __syncthreads();  // the previous chunk's fragments have been read
+    for (int t = threadIdx.x; t < kCI * kTcHalo; t += blockDim.x) {
+      const int ci = t / kTcHalo, pix = t - ci * kTcHalo;
+      const int yy = pix / (kCT + 2), xx = pix - yy * (kCT + 2);
+      const int y = ty0 + yy - 1, x = tx0 + xx - 1;
+      const int c = c0 + ci;
+      float v = 0.f;
+      if (c < cin && y >= 0 && y < g.H && x >= 0 && x < g.W) {
+        if (c < g.ca) {
+          const int sy = g.a_up ? y >> 1 : y, sx = g.a_up ? x >> 1 : x;
+          const size_t idx = (((size_t)n * g.ca + c) * ha + sy) * wa + sx;
+          v = g.a[idx];
+          if (g.amask && !(g.amask[idx] > 0.f)) v = 0.f;
+        } else {
+          v = g.b[(((size_t)n * g.cb + (c - g.ca)) * g.H + y) * g.W + x];
+        }
+      }
+      const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+      const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+      s_x16[(size_t)pix * (2 * kTcRow) + ci] = hi;
+      s_x16[(size_t)(kTcHalo + pix) * (2 * kTcRow) + ci] = lo;
+    }
+    for (int t = threadIdx.x; t < 9 * CO * kCI; t += blockDim.x) {
+      const int ci = t % kCI, r = t / kCI, co = r % CO, tap = r / CO;
+      __nv_bfloat16 w = __float2bfloat16_rn(0.f);
+      if (co0 + co < g.cout && c0 + ci < cin) w = g.w[((size_t)(co0 + co) * cin + c0 + ci) * 9 + tap];
+      s_w16[(size_t)(tap * CO + co) * (2 * kTcRow) + ci] = w;
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int tap = 0; tap < 9; ++tap) {
+      const int ky = tap / 3, kx = tap - ky * 3;
+      uint32_t a[MT][4];
+#pragma unroll
+      for (int m = 0; m < MT; ++m) {
+        const uint32_t* w0 = s_w + (size_t)(tap * CO + m * 16 + gid) * kTcRow + tig;
+        const uint32_t* w8 = w0 + 8 * kTcRow;
+        a[m][0] = w0[0];
+        a[m][1] = w8[0];
+        a[m][2] = w0[4];
+        a[m][3] = w8[4];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int row = 2 * warp + (j >> 1), x0 = (j & 1) * 8;
+        const int hp = (row + ky) * (kCT + 2) + x0 + gid + kx;
+#pragma unroll
+        for (int pl = 0; pl < 2; ++pl) {
+          const uint32_t* bx = s_x + (size_t)(pl * kTcHalo + hp) * kTcRow + tig;
+          const uint32_t b0 = bx[0], b1 = bx[4];
+#pragma unroll
+          for (int m = 0; m < MT; ++m) mma_bf16_16816(acc[m][j], a[m], b0, b1);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < MT; ++m)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int y = ty0 + 2 * warp + (j >> 1);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int co = co0 + m * 16 + gid + (e >> 1) * 8;
+        const int x = tx0 + (j & 1) * 8 + tig * 2 + (e & 1);
+        if (co >= g.cout || y >= g.H || x >= g.W) continue;
+        float v = acc[m][j][e] + (g.bias ? g.bias[co] : 0.f);
+        if (g.relu) v = fmaxf(v, 0.f);
+        float* o = g.out + (((size_t)n * g.cout + co) * g.H + y) * g.W + x;
+        *o = g.accumulate ? *o + v : v;
+      }
+    }
+}
+
+template <int MT> constexpr size_t conv_tc_smem() { return sizeof(uint32_t) * (2 * kTcHalo + 9 * 16 * MT) * kTcRow; }
 
 // weights of the backward-data convolution: wt[ci][co][k] = w[co][ci][8 - k]
 __global__ void k_flip_transpose(const __nv_bfloat16* __restrict__ w, int cout, int cin,
@@ -445,6 +571,7 @@ struct Net {
   Mem pool[3], gpool[3], gup, gin_tmp, out, sq, gpre, lossv, tgt;
   cudaStream_t s = nullptr;
   long step = 0;
+  bool cuda_cores = false;  // FP32 CUDA-core convolutions instead of the tensor cores
 
   int lvH(int l) const { return H >> l; }
   int lvW(int l) const { return W >> l; }
@@ -533,6 +660,8 @@ struct Net {
     tgt.alloc(sizeof(float) * (size_t)nmax * H * W);
     lossv.alloc(sizeof(float));
     UN_CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    const char* cc = getenv("MFISTA_UNET_CUDA_CORES");
+    cuda_cores = cc && cc[0] == '1';
     UN_CK(cudaDeviceSynchronize());  // the set-up above ran on the legacy stream
     init_params(1234);
   }
@@ -580,13 +709,29 @@ struct Net {
   float* src_a_grad(int i) const { return kSrcA[i] <= -2 ? gpool[-kSrcA[i] - 2].as<float>() : gact[kSrcA[i]].as<float>(); }
   const float* src_b_ptr(int i) const { return src_b(i) >= 0 ? act[src_b(i)].as<float>() : nullptr; }
 
+  // a 3x3 convolution on the tensor cores (32 output channels per CTA, 16
+  // when cout is 16); MFISTA_UNET_CUDA_CORES=1 selects the FP32 CUDA-core
+  // kernel instead (comparison runs)
+  void conv(const ConvArgs& a, int n) {
+    dim3 grid(cdiv(a.W, kCT) * cdiv(a.H, kCT), 1, n);
+    if (cuda_cores) {
+      grid.y = cdiv(a.cout, kCO);
+      k_conv3x3<<<grid, 128, 0, s>>>(a);
+    } else if (a.cout % 32 == 0) {
+      grid.y = a.cout / 32;
+      k_conv3x3_tc<2><<<grid, 256, conv_tc_smem<2>(), s>>>(a);
+    } else {
+      grid.y = cdiv(a.cout, 16);
+      k_conv3x3_tc<1><<<grid, 256, conv_tc_smem<1>(), s>>>(a);
+    }
+    UN_LAUNCH();
+  }
+
   void conv_forward(int i, int n) {
     const Conv& c = convs[i];
     ConvArgs ga{src_a_ptr(i), nullptr, c.ca, c.a_up, src_b_ptr(i), c.cb, wb(c), p.as<float>() + c.b_off,
                 act[i + 1].as<float>(), c.cout, lvH(c.level), lvW(c.level), 1, 0};
-    dim3 grid(cdiv(ga.W, kCT) * cdiv(ga.H, kCT), cdiv(c.cout, kCO), n);
-    k_conv3x3<<<grid, 128, 0, s>>>(ga);
-    UN_LAUNCH();
+    conv(ga, n);
   }
 
   void pool_forward(int l, int n) {  // pool l of e_{l+1} = act[2 + 2 l]
@@ -643,9 +788,7 @@ struct Net {
     UN_LAUNCH();
     float* gi = c.a_up ? gup.as<float>() : gin_tmp.as<float>();  // w.r.t. the (upsampled) concat input
     ConvArgs gd{go, mask, c.cout, 0, nullptr, 0, wt.as<__nv_bfloat16>(), nullptr, gi, cin, Hl, Wl, 0, 0};
-    dim3 grid(cdiv(Wl, kCT) * cdiv(Hl, kCT), cdiv(cin, kCO), n);
-    k_conv3x3<<<grid, 128, 0, s>>>(gd);
-    UN_LAUNCH();
+    conv(gd, n);
     float* ga_dst = src_a_grad(i);
     const size_t hw = (size_t)Hl * Wl;
     if (c.a_up) {  // sum the 2x2 blocks into a's half-resolution gradient

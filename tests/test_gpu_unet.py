@@ -1,9 +1,10 @@
 """The warm-start U-Net's GPU kernels against the CPU oracle.
 
-Forward outputs within 1e-5 relative L2 of the oracle (the GPU sums in
-FP32, the oracle in float64, both with the same BF16-rounded weights) and
-parameter gradients within 1e-4; training steps lower the loss and are
-deterministic."""
+Forward outputs within 1e-5 relative L2 of the oracle (the GPU convolves on
+the tensor cores with BF16 weights and the activations split into two BF16
+planes, accumulating in FP32; the oracle in float64, both with the same
+BF16-rounded weights) and parameter gradients within 1e-4; training steps
+lower the loss and are deterministic."""
 import numpy as np
 import pytest
 
@@ -67,3 +68,25 @@ def test_unet_rejects_bad_shapes(gpulib):
     assert L.mfista_unet_forward(net.h, warmstart._fp(x), 3, warmstart._fp(out)) == 2  # batch above its maximum
     assert L.mfista_unet_forward(net.h, warmstart._fp(x), 0, warmstart._fp(out)) == 2
     net.close()
+
+
+def test_tensor_core_convolutions_match_cuda_core_ones(gpulib, monkeypatch):
+    """The tensor-core convolutions (default) and the FP32 CUDA-core ones
+    (MFISTA_UNET_CUDA_CORES=1) give the same network output to 1e-5 on a
+    64 x 64 batch, every level and both channel widths of the kernel."""
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((3, 2, 64, 64)).astype(np.float32)
+    outs = []
+    for cc in ("0", "1"):
+        monkeypatch.setenv("MFISTA_UNET_CUDA_CORES", cc)
+        net = _net(64, 3)
+        p = net.params()
+        lay, hw, hb, n = U.layout()
+        p[hw:] = np.abs(p[hw:])
+        net.set_params(p)
+        outs.append(net.forward(x))
+        _, g = net.grad(x, np.abs(x[:, 0]))
+        outs.append(g)
+        net.close()
+    assert rel(outs[0], outs[2]) < 1e-5
+    assert rel(outs[1], outs[3]) < 1e-4
