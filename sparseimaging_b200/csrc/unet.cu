@@ -370,6 +370,113 @@ __global__ void __launch_bounds__(256) k_conv3x3_wgrad(WgradArgs g) {
   }
 }
 
+// The weight gradient on the tensor cores: per 16 x 16 pixel tile,
+//   part[tile][co][ci][tap] = sum_{pix} G[co][pix] X[ci][pix + tap],
+// a GEMM with M = 16 output channels, N = 16 input channels per tap and
+// K = the tile's 256 pixels (16 k16 steps, one pixel row each).  G (the
+// masked output gradient) and X (the input, as in k_conv3x3) are FP32 and
+// enter as BF16 hi/lo planes; the three products hi*hi + hi*lo + lo*hi are
+// accumulated in FP32 (lo*lo, ~2^-18 of the rest, is left out).  Nine warps,
+// one per tap; the partials go to the same layout as k_conv3x3_wgrad's and
+// are reduced over tiles in tile order by k_reduce_partials.
+constexpr int kWgG = 132;  // 32-bit words per staged G row (256 pixels + pad)
+constexpr int kWgX = 164;  // 32-bit words per staged X channel (324 halo pixels + pad)
+
+__global__ void __launch_bounds__(288) k_conv3x3_wgrad_tc(WgradArgs g) {
+  extern __shared__ __align__(16) uint32_t s_wg[];
+  uint32_t* s_g = s_wg;                   // [2][16][kWgG]
+  uint32_t* s_x = s_wg + 2 * 16 * kWgG;   // [2][16][kWgX]
+  __nv_bfloat16* s_g16 = reinterpret_cast<__nv_bfloat16*>(s_g);
+  __nv_bfloat16* s_x16 = reinterpret_cast<__nv_bfloat16*>(s_x);
+  const int tiles_x = cdiv(g.W, kCT), tiles_y = cdiv(g.H, kCT);
+  const int tile = blockIdx.x;  // over n * tiles
+  const int n = tile / (tiles_x * tiles_y), tr = tile - n * tiles_x * tiles_y;
+  const int tx0 = (tr % tiles_x) * kCT, ty0 = (tr / tiles_x) * kCT;
+  const int co0 = blockIdx.y * 16, ci0 = blockIdx.z * kCI;
+  const int cin = g.ca + g.cb;
+  const int ha = g.a_up ? g.H / 2 : g.H, wa = g.a_up ? g.W / 2 : g.W;
+  for (int t = threadIdx.x; t < 16 * kCT * kCT; t += blockDim.x) {
+    const int co = t / (kCT * kCT), p = t - co * kCT * kCT;
+    const int y = ty0 + p / kCT, x = tx0 + p % kCT;
+    float v = 0.f;
+    if (co0 + co < g.cout && y < g.H && x < g.W) {
+      const size_t idx = (((size_t)n * g.cout + co0 + co) * g.H + y) * g.W + x;
+      v = g.g[idx];
+      if (g.gmask && !(g.gmask[idx] > 0.f)) v = 0.f;
+    }
+    const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+    s_g16[(size_t)co * (2 * kWgG) + p] = hi;
+    s_g16[(size_t)(16 + co) * (2 * kWgG) + p] = __float2bfloat16_rn(v - __bfloat162float(hi));
+  }
+  for (int t = threadIdx.x; t < kCI * kTcHalo; t += blockDim.x) {
+    const int ci = t / kTcHalo, pix = t - ci * kTcHalo;
+    const int yy = pix / (kCT + 2), xx = pix - yy * (kCT + 2);
+    const int y = ty0 + yy - 1, x = tx0 + xx - 1;
+    const int c = ci0 + ci;
+    float v = 0.f;
+    if (c < cin && y >= 0 && y < g.H && x >= 0 && x < g.W) {
+      if (c < g.ca) {
+        const int sy = g.a_up ? y >> 1 : y, sx = g.a_up ? x >> 1 : x;
+        v = g.a[(((size_t)n * g.ca + c) * ha + sy) * wa + sx];
+      } else {
+        v = g.b[(((size_t)n * g.cb + (c - g.ca)) * g.H + y) * g.W + x];
+      }
+    }
+    const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+    s_x16[(size_t)ci * (2 * kWgX) + pix] = hi;
+    s_x16[(size_t)(16 + ci) * (2 * kWgX) + pix] = __float2bfloat16_rn(v - __bfloat162float(hi));
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, tap = threadIdx.x >> 5;  // warp = tap
+  const int gid = lane >> 2, tig = lane & 3;
+  const int ky = tap / 3, kx = tap - ky * 3;
+  float acc[2][4];
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[j][e] = 0.f;
+  auto pack = [](__nv_bfloat16 lo16, __nv_bfloat16 hi16) -> uint32_t {
+    return (uint32_t)__bfloat16_as_ushort(lo16) | ((uint32_t)__bfloat16_as_ushort(hi16) << 16);
+  };
+#pragma unroll 1
+  for (int py = 0; py < kCT; ++py) {  // k16 step: pixels (py, 0..15)
+    uint32_t a[2][4];                   // G planes: rows co = gid (+8), k = pixel
+#pragma unroll
+    for (int pl = 0; pl < 2; ++pl) {
+      const uint32_t* r0 = s_g + (size_t)(pl * 16 + gid) * kWgG + py * (kCT / 2) + tig;
+      const uint32_t* r8 = r0 + 8 * kWgG;
+      a[pl][0] = r0[0];
+      a[pl][1] = r8[0];
+      a[pl][2] = r0[4];
+      a[pl][3] = r8[4];
+    }
+    const int hrow = (py + ky) * (kCT + 2) + kx;  // halo index of pixel (py, 0) shifted by the tap
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {  // n8 tiles: input channels 8j .. 8j+7
+      uint32_t b[2][2];
+#pragma unroll
+      for (int pl = 0; pl < 2; ++pl) {
+        const __nv_bfloat16* xr = s_x16 + (size_t)(pl * 16 + 8 * j + gid) * (2 * kWgX) + hrow;
+        b[pl][0] = pack(xr[tig * 2], xr[tig * 2 + 1]);
+        b[pl][1] = pack(xr[tig * 2 + 8], xr[tig * 2 + 9]);
+      }
+      mma_bf16_16816(acc[j], a[0], b[0][0], b[0][1]);  // hi * hi
+      mma_bf16_16816(acc[j], a[0], b[1][0], b[1][1]);  // hi * lo
+      mma_bf16_16816(acc[j], a[1], b[0][0], b[0][1]);  // lo * hi
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 2; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int co = co0 + gid + (e >> 1) * 8, ci = ci0 + 8 * j + tig * 2 + (e & 1);
+      if (co < g.cout && ci < cin)
+        g.part[(((size_t)tile * g.cout + co) * cin + ci) * 9 + tap] = acc[j][e];
+    }
+}
+
+constexpr size_t kWgradTcSmem = sizeof(uint32_t) * (2 * 16 * kWgG + 2 * 16 * kWgX);
+
 // out[i] = sum_t part[t][i] (t ascending), i < len
 __global__ void k_reduce_partials(const float* __restrict__ part, int ntiles, long len, float* __restrict__ out) {
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -775,7 +882,10 @@ struct Net {
     const float* mask = act[i + 1].as<float>();  // ReLU: the gradient passes where the output > 0
     const int ntiles = n * cdiv(Hl, kCT) * cdiv(Wl, kCT);
     WgradArgs wa{go, mask, src_a_ptr(i), c.ca, c.a_up, src_b_ptr(i), c.cb, part.as<float>(), c.cout, Hl, Wl};
-    k_conv3x3_wgrad<<<dim3(ntiles, cdiv(c.cout, kCO), cdiv(cin, kCI)), 256, 0, s>>>(wa);
+    if (cuda_cores)
+      k_conv3x3_wgrad<<<dim3(ntiles, cdiv(c.cout, kCO), cdiv(cin, kCI)), 256, 0, s>>>(wa);
+    else
+      k_conv3x3_wgrad_tc<<<dim3(ntiles, cdiv(c.cout, 16), cdiv(cin, kCI)), 288, kWgradTcSmem, s>>>(wa);
     UN_LAUNCH();
     const long len = (long)c.cout * cin * 9;
     k_reduce_partials<<<cdiv(len, 256), 256, 0, s>>>(part.as<float>(), ntiles, len, g.as<float>() + c.w_off);
