@@ -183,11 +183,82 @@ def training_problem(seed, nx=128):
     return synth.lambda_grid_problem(seed=seed, nx=nx, n_stations=int(rng.integers(8, 13)), n_hours=180)
 
 
-def make_training_set(seeds, nx=128, iters=1500, batch=32, lam_rel=TRAIN_LAMBDA):
+_C4 = {}
+
+
+def config4_geometry(nx=256):
+    """The uv coverage of the learned-warm-start configuration, shared by
+    all its skies: 12 stations (seeded) over 303 hour angles, 66 baselines,
+    M = 19998 points; with the Lipschitz constant of A^H A (unit weights),
+    and the network's dirty-beam channel (the beam over its peak), which a
+    shared coverage with uniform weights makes the same for every sky."""
+    if nx not in _C4:
+        from . import nufft_lipschitz
+        u, v = synth.earth_rotation_uv(12, 303, seed=4)
+        u_dx, v_dy = synth.scale_uv_to_radians(u, v, nx, synth.safe_kmax(nx))
+        ones = np.ones(u_dx.size)
+        lip1 = nufft_lipschitz(u_dx, v_dy, ones, nx, nx, iters=30)
+        beam = nufft_adjoint(u_dx, v_dy, nx, nx, ones, np.zeros_like(ones))
+        _C4[nx] = (u_dx, v_dy, lip1, (beam / beam.max()).reshape(nx, nx))
+    return _C4[nx]
+
+
+def config4_problem(seed, nx=256):
+    """A config-4 problem: the seeded training sky (3-12 blobs, sigma 1-10
+    px, a ring or crescent with probability 0.5, flux 1) seen through the
+    shared coverage (config4_geometry), visibilities from this library's
+    FP64 NUFFT (~1e-12 of the exact DFT) plus complex noise of 1 % of
+    max|V|."""
+    from . import nufft_forward
+    u_dx, v_dy, _, _ = config4_geometry(nx)
+    sky = synth.sky_training(nx, seed)
+    fr, fi = nufft_forward(u_dx, v_dy, nx, nx, sky.ravel())
+    vis = fr + 1j * fi
+    sigma = 0.01 * float(np.abs(vis).max())
+    rng = np.random.default_rng(seed + 7777)
+    vis = vis + sigma * (rng.standard_normal(vis.size) + 1j * rng.standard_normal(vis.size))
+    return synth.NufftProblem(u_dx, v_dy, vis.real.copy(), vis.imag.copy(), np.full(vis.size, sigma), nx, nx, sky)
+
+
+def _batch_setup(ps, nx, lam_rel):
+    """Network inputs, scales and MFISTA parameters of config-4 problems
+    (shared coverage, uniform weights per problem: cinit = L_unit / sigma^2)."""
+    _, _, lip1, beam = config4_geometry(nx)
+    X, scales, problems = [], [], []
+    for p in ps:
+        sig = float(p.vis_std[0])
+        w2 = 1.0 / sig ** 2
+        g0 = nufft_adjoint(p.u_dx, p.v_dy, nx, nx, p.vis_r * w2, p.vis_i * w2)
+        lam = lam_rel * float(np.abs(g0).max())
+        # dirty image over the beam's peak (M w^2), then over its own peak
+        dirty = g0.reshape(nx, nx) / (p.m * w2)
+        scale = max(float(np.abs(dirty).max()), 1e-30)
+        X.append(np.stack([dirty / scale, beam]).astype(np.float32))
+        scales.append(scale)
+        problems.append(dict(lambda_l1=lam, lambda_tsv=lam, cinit=lip1 * w2, nonneg_flag=1))
+    cat = lambda f: np.concatenate([getattr(p, f) for p in ps])
+    off = np.concatenate([[0], np.cumsum([p.m for p in ps])]).astype(np.int32)
+    geo = (cat("u_dx"), cat("v_dy"), cat("vis_r"), cat("vis_i"), cat("vis_std"), nx, nx)
+    return X, scales, problems, geo, off
+
+
+def make_training_set(seeds, nx=128, iters=1500, batch=32, lam_rel=TRAIN_LAMBDA, problem=None, eps=1e-7):
     """(inputs [n][2][nx][nx], targets [n][nx][nx]) for the given seeds: the
-    targets are FP64 MFISTA solutions (`iters` iterations) at
+    targets are FP64 MFISTA solutions (at most `iters` iterations, the
+    reference's stopping rule with `eps`) at
     lambda_l1 = lambda_tsv = lam_rel * max|A^H W^2 y|."""
     from . import FP64, nufft_batch, nufft_lipschitz
+    if problem is not None:
+        X, T = [], []
+        for i in range(0, len(seeds), batch):
+            ps = [problem(s) for s in seeds[i:i + batch]]
+            Xb, scales, problems, geo, off = _batch_setup(ps, nx, lam_rel)
+            for q in problems:
+                q["maxiter"] = iters
+            Xs, _ = nufft_batch(*geo, problems, eps, pt_off=off, precision=FP64)
+            X += Xb
+            T += [(Xs[k].reshape(nx, nx) / sc).astype(np.float32) for k, sc in enumerate(scales)]
+        return np.stack(X), np.stack(T)
     X, T = [], []
     for i in range(0, len(seeds), batch):
         ps = [training_problem(s, nx) for s in seeds[i:i + batch]]
@@ -224,6 +295,87 @@ def train(X, T, steps=400, batch=8, lr=1e-3, seed=0, net=None, log=None):
     return net, hist
 
 
+def evaluate(net, seeds, nx=256, batch=64, lam_rel=TRAIN_LAMBDA, fstar_iters=6000, precision=None,
+             problem=None):
+    """Held-out evaluation: per seed, F* and x* from a long FP64 solve
+    (`fstar_iters` iterations, stopping rule off), then MFISTA to
+    F*(1 + 1e-6) from zero and from the network's start (where its objective
+    is below the zero image's, choose_starts).  Returns per-problem
+    iterations, batch solve times and relative image errors against x*."""
+    from . import FP64, nufft_batch
+    problem = problem or config4_problem
+    prec = FP64 if precision is None else precision
+    out = {"iters_zero": [], "iters_warm": [], "err_zero": [], "err_warm": [], "used": [], "s_zero": 0.0,
+           "s_warm": 0.0, "s_predict": 0.0, "reached_zero": 0, "reached_warm": 0}
+    for i in range(0, len(seeds), batch):
+        ps = [problem(s) for s in seeds[i:i + batch]]
+        X, scales, problems, geo, off = _batch_setup(ps, nx, lam_rel)
+        long = [dict(q, maxiter=fstar_iters) for q in problems]
+        Xs, Rs = nufft_batch(*geo, long, 0.0, pt_off=off, precision=FP64)
+        targets = [r["finalcost"] * (1 + 1e-6) for r in Rs]
+        timed = [dict(q, maxiter=fstar_iters, target_cost=t) for q, t in zip(problems, targets)]
+        t0 = time.perf_counter()
+        Xz, Rz = nufft_batch(*geo, timed, 0.0, pt_off=off, precision=prec)
+        out["s_zero"] += time.perf_counter() - t0
+        t0 = time.perf_counter()
+        pred = net.forward(np.stack(X))
+        x0 = np.concatenate([pred[k].reshape(-1).astype(np.float64) * sc for k, sc in enumerate(scales)])
+        # per problem, the start whose objective is lower (one evaluation each)
+        at0 = [dict(q, maxiter=0, target_cost=0.0) for q in problems]
+        _, Rw0 = nufft_batch(*geo, at0, 0.0, pt_off=off, precision=prec, xinit=x0)
+        _, Rz0 = nufft_batch(*geo, at0, 0.0, pt_off=off, precision=prec)
+        used = np.array([a["finalcost"] < b["finalcost"] for a, b in zip(Rw0, Rz0)])
+        starts = np.where(used[:, None], x0.reshape(len(ps), -1), 0.0).reshape(-1)
+        out["s_predict"] += time.perf_counter() - t0
+        t0 = time.perf_counter()
+        Xw, Rw = nufft_batch(*geo, timed, 0.0, pt_off=off, precision=prec, xinit=starts)
+        out["s_warm"] += time.perf_counter() - t0
+        for k in range(len(ps)):
+            nrm = max(np.linalg.norm(Xs[k]), 1e-300)
+            out["err_zero"].append(float(np.linalg.norm(Xz[k] - Xs[k]) / nrm))
+            out["err_warm"].append(float(np.linalg.norm(Xw[k] - Xs[k]) / nrm))
+        out["iters_zero"] += [r["ITER"] for r in Rz]
+        out["iters_warm"] += [r["ITER"] for r in Rw]
+        out["reached_zero"] += int(sum(r["finalcost"] <= t for r, t in zip(Rz, targets)))
+        out["reached_warm"] += int(sum(r["finalcost"] <= t for r, t in zip(Rw, targets)))
+        out["used"] += used.tolist()
+    n = len(out["iters_zero"])
+    out["summary"] = {
+        "problems": n, "used_start": int(sum(out["used"])),
+        "mean_iters_zero": float(np.mean(out["iters_zero"])), "mean_iters_warm": float(np.mean(out["iters_warm"])),
+        "median_iters_zero": float(np.median(out["iters_zero"])),
+        "median_iters_warm": float(np.median(out["iters_warm"])),
+        "solves_per_s_zero": n / out["s_zero"], "solves_per_s_warm": n / (out["s_warm"] + out["s_predict"]),
+        "median_img_err_zero": float(np.median(out["err_zero"])),
+        "median_img_err_warm": float(np.median(out["err_warm"])),
+        "reached_zero": out["reached_zero"], "reached_warm": out["reached_warm"]}
+    return out
+
+
+def config4_main(n_train, n_eval, steps, out_weights, out_json, train_iters=5000):
+    """Config 4 end to end on one GPU: training set (FP64 solves, reference
+    stopping rule at eps 1e-6), training, held-out evaluation."""
+    t0 = time.time()
+    seeds_train = list(range(20000, 20000 + n_train))
+    seeds_eval = list(range(90000, 90000 + n_eval))
+    X, T = make_training_set(seeds_train, nx=256, iters=train_iters, batch=64, problem=config4_problem, eps=1e-6)
+    t1 = time.time()
+    net, hist = train(X, T, steps=steps, batch=8, log=print)
+    t2 = time.time()
+    os.makedirs(os.path.dirname(os.path.abspath(out_weights)), exist_ok=True)
+    np.save(out_weights, net.params())
+    ev = evaluate(net, seeds_eval, nx=256)
+    t3 = time.time()
+    res = {"config": "256x256, M = 19998 (12 stations x 303 hour angles), lambda_l1 = lambda_tsv = "
+                     f"{TRAIN_LAMBDA} max|A^H W^2 y|, targets: FP64 MFISTA to eps 1e-6",
+           "n_train": n_train, "n_eval": n_eval, "steps": steps, "data_s": t1 - t0, "train_s": t2 - t1,
+           "eval_s": t3 - t2, "loss_first": hist[0], "loss_last": float(np.mean(hist[-50:])),
+           "eval": ev["summary"],
+           "per_problem": {k: ev[k] for k in ("iters_zero", "iters_warm", "err_zero", "err_warm", "used")}}
+    json.dump(res, open(out_json, "w"), indent=1)
+    print(json.dumps({k: v for k, v in res.items() if k != "per_problem"}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--train", action="store_true")
@@ -232,8 +384,16 @@ def main():
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--iters", type=int, default=1500, help="FP64 MFISTA iterations per training target")
     ap.add_argument("--lam", type=float, default=TRAIN_LAMBDA, help="training lambdas relative to max|A^H W^2 y|")
+    ap.add_argument("--config4", action="store_true",
+                    help="256x256 / M = 19998 configuration: training set, training and held-out evaluation")
+    ap.add_argument("--n-eval", type=int, default=256)
+    ap.add_argument("--json", default="warmstart_config4.json")
     a = ap.parse_args()
     os.environ.setdefault("MFISTA_QUIET", "1")
+    if a.config4:
+        out = a.out if a.out != WEIGHTS else os.path.join(HERE, "data", "unet_warmstart_256.npy")
+        config4_main(a.n_train, a.n_eval, a.steps, out, a.json)
+        return
     if not a.train:
         ap.print_help()
         return
