@@ -781,6 +781,176 @@ __global__ void __launch_bounds__(256, GroupChunk<T>::kMinBlocks) k_nufft_interp
   }
 }
 
+// The same grouped interpolation with the taps formed on the fly instead of
+// held in registers: a lane walks its 18 taps t = lane + 32 s as (lx, ly)
+// pairs, takes the weight wy[ly] wx[lx] from the warp's copy of the point's
+// 48 tap factors in shared memory, and the cell from (mx, my) (a direct,
+// inside point, the usual case, needs no per-tap tests: its rows only wrap
+// at kx = 0).  Far fewer registers per thread (more warps per SM to hide
+// the gathers) for a little more arithmetic per tap; the products and their
+// order are those of k_nufft_interp_group, so results are bit-identical.
+template <typename T> struct TapPoint {
+  int k, mx0, my0;  // point, mx - 11, my - 11
+  bool plain;       // every tap direct and inside the grid
+  double w, vr, vi;
+};
+
+template <typename T, int G>
+__device__ __forceinline__ void interp_group_fly(const TapPoint<T>& P, const T* __restrict__ swx,
+                                                 const T* __restrict__ swy, const cplx<T>* __restrict__ gall,
+                                                 long gstride, const int* list, int pos, int lane, int nx, int ny,
+                                                 double inv_mm, const NufftGeom<T>& geo,
+                                                 const double2* __restrict__ ax_base, double2* __restrict__ ax_out,
+                                                 cplx<T>* __restrict__ y2, double* s_chi_w) {
+  constexpr int V = (G == 8) ? 4 : (G == 4) ? 3 : (G == 2) ? 2 : 1;
+  constexpr int NT = (kTaps * kTaps) / 32;
+  const cplx<T>* g[G];
+#pragma unroll
+  for (int i = 0; i < G; ++i) g[i] = gall + (size_t)list[pos + i] * gstride;
+  T acc[2 * G];
+#pragma unroll
+  for (int i = 0; i < 2 * G; ++i) acc[i] = 0;
+  int lx = lane / kTaps, ly = lane - (lane / kTaps) * kTaps;
+  if (P.plain) {
+#pragma unroll 2
+    for (int s = 0; s < NT; ++s) {
+      const int kx = P.mx0 + lx;
+      const int cc = (kx + (kx < 0 ? 2 * nx : 0)) * (ny + 1) + P.my0 + ly;
+      const T wg = swy[ly] * swx[lx];
+#pragma unroll
+      for (int i = 0; i < G; ++i) {
+        const cplx<T> gv = g[i][cc];
+        acc[i] += gv.x * wg;
+        acc[G + i] += (-gv.y) * wg;  // NU_SIGN: direct taps only
+      }
+      ly += 32 - kTaps;  // t += 32 = one row of 24 taps and 8 more
+      lx += 1;
+      if (ly >= kTaps) {
+        ly -= kTaps;
+        lx += 1;
+      }
+    }
+  } else {
+#pragma unroll 1
+    for (int s = 0; s < NT; ++s) {
+      const int m = P.my0 + ly, mxm = P.mx0 + lx;
+      int col = half_col(m, ny), row;
+      bool mir = false;
+      if (col >= 0) {
+        row = wrap_row(mxm, nx);
+      } else {
+        col = half_col(-m, ny);
+        row = wrap_row(-mxm, nx);
+        mir = true;
+      }
+      if (col >= 0 && row >= 0) {
+        const int cc = row * (ny + 1) + col;
+        const T wg = swy[ly] * swx[lx];
+#pragma unroll
+        for (int i = 0; i < G; ++i) {
+          const cplx<T> gv = g[i][cc];
+          acc[i] += gv.x * wg;
+          // NU_SIGN on the imaginary part of direct taps, + on mirrored ones
+          acc[G + i] += (mir ? gv.y : -gv.y) * wg;
+        }
+      }
+      ly += 32 - kTaps;
+      lx += 1;
+      if (ly >= kTaps) {
+        ly -= kTaps;
+        lx += 1;
+      }
+    }
+  }
+  transpose_reduce<V>(acc, lane);
+  const T im = __shfl_xor_sync(0xffffffffu, acc[0], 16);
+  const int fin = lane >> (5 - V);
+  if (lane < 16 && (lane & ((1 << (5 - V)) - 1)) == 0) {
+    const int slot = pos + fin;
+    const int b = list[slot];
+    double fr = (double)acc[0] * inv_mm, fi = (double)im * inv_mm;
+    const size_t e = (size_t)b * geo.y2_bstride + P.k;
+    if (ax_base) {
+      fr += ax_base[e].x;
+      fi += ax_base[e].y;
+    }
+    if (ax_out) ax_out[e] = make_double2(fr, fi);
+    const double rr = (P.vr - fr) * P.w;
+    const double ri = (P.vi - fi) * P.w;
+    s_chi_w[slot] += rr * rr + ri * ri;
+    if (y2) y2[e] = mk<T>((T)(rr * P.w), (T)(ri * P.w));
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 3) k_nufft_interp_group_fly(
+    NufftGeom<T> geo, const cplx<T>* __restrict__ gall, long gstride, int nx, int ny, double inv_mm,
+    const ProbState* __restrict__ st, int gate, Partials part, int qchi, cplx<T>* __restrict__ y2, int B,
+    const double2* __restrict__ ax_base, double2* __restrict__ ax_out, int ppw) {
+  constexpr int PB = SharedChunk<T>::kInterp;
+  constexpr int GM = GroupChunk<T>::kGmax;
+  __shared__ double s_chi[8][PB];
+  __shared__ int s_list[PB];
+  __shared__ int s_cnt[8];
+  __shared__ T s_wt[8][2][kTaps];  // per warp: the point's wx, wy
+  const int nact = active_chunk<PB>(st, gate, B, blockIdx.y, s_list, s_cnt);
+  if (nact == 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int mtot = geo.pt_hi[0];
+  if (lane < PB) s_chi[warp][lane] = 0.0;
+  __syncwarp();
+  for (int q = 0; q < ppw; ++q) {
+    TapPoint<T> P;
+    P.k = (blockIdx.x * 8 + warp) * ppw + q;
+    if (P.k >= mtot) break;
+    const int k = P.k;
+    const int mxk = geo.mx[k], myk = geo.my[k];
+    if (lane < kTaps) {
+      s_wt[warp][0][lane] = geo.wx[(size_t)k * kTaps + lane];
+      s_wt[warp][1][lane] = geo.wy[(size_t)k * kTaps + lane];
+    }
+    P.mx0 = mxk - (kMSP - 1);
+    P.my0 = myk - (kMSP - 1);
+    // direct (0 <= ky < Ny) and inside (-Nx <= kx < Nx) for every tap
+    P.plain = P.my0 >= 0 && myk + kMSP < ny && P.mx0 >= -nx && mxk + kMSP < nx;
+    P.w = geo.weight[k];
+    P.vr = geo.vis_r[k];
+    P.vi = geo.vis_i[k];
+    __syncwarp();
+    const T* swx = s_wt[warp][0];
+    const T* swy = s_wt[warp][1];
+    int pos = 0;
+    while (pos < nact) {
+      const int rem = nact - pos;
+      if (GM >= 8 && rem >= 8) {
+        interp_group_fly<T, (GM >= 8 ? 8 : 1)>(P, swx, swy, gall, gstride, s_list, pos, lane, nx, ny, inv_mm, geo,
+                                               ax_base, ax_out, y2, s_chi[warp]);
+        pos += 8;
+      } else if (GM >= 4 && rem >= 4) {
+        interp_group_fly<T, (GM >= 4 ? 4 : 1)>(P, swx, swy, gall, gstride, s_list, pos, lane, nx, ny, inv_mm, geo,
+                                               ax_base, ax_out, y2, s_chi[warp]);
+        pos += 4;
+      } else if (rem >= 2) {
+        interp_group_fly<T, 2>(P, swx, swy, gall, gstride, s_list, pos, lane, nx, ny, inv_mm, geo, ax_base, ax_out,
+                               y2, s_chi[warp]);
+        pos += 2;
+      } else {
+        interp_group_fly<T, 1>(P, swx, swy, gall, gstride, s_list, pos, lane, nx, ny, inv_mm, geo, ax_base, ax_out,
+                               y2, s_chi[warp]);
+        pos += 1;
+      }
+    }
+    __syncwarp();  // the next point's factors overwrite s_wt[warp]
+  }
+  __syncthreads();
+  if (threadIdx.x < nact && qchi >= 0) {
+    double c = 0.0;
+#pragma unroll
+    for (int wp = 0; wp < 8; ++wp) c += s_chi[wp][threadIdx.x];
+    part.at(qchi, s_list[threadIdx.x])[blockIdx.x] = c;
+  }
+}
+
 // spreading: one thread-block cluster per (16 x 16 tile, problem chunk); one
 // thread per cell holding the chunk's accumulators.  The tile's point list is
 // split into contiguous segments, one per CTA of the cluster, which bounds

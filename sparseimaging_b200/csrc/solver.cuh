@@ -252,11 +252,15 @@ template <typename T> struct NufftOp : Op {
   int rpc = 8, cpc = 8, tile_r = 8, tile_c = 32, ntiles = 0;
   int ippw = SharedChunk<T>::kInterpPts;  // interpolation points per warp (shared geometry)
   int spread_cs = 8;                      // spreading cluster size (shared geometry)
+  // FP32 grouped interpolation with taps formed on the fly (fewer registers)
+  // instead of held in registers; both give the same bits
+  bool interp_fly = false;
   size_t smem_rows = 0, smem_cols = 0;
   long gstride = 0;
   double inv_mm = 0;
 
   NufftOp(Ctx& ctx, const NufftInput& in, bool correct = false) : c(ctx) {
+    if (const char* f = getenv("MFISTA_INTERP_FLY")) interp_fly = f[0] == '1';
     nx = in.Nx;
     ny = in.Ny;
     B = ctx.B;
@@ -391,9 +395,14 @@ template <typename T> struct NufftOp : Op {
     // FP32: grouped kernel; FP64 (register-bound with 2G double sums): one
     // problem at a time.  Both chunk the batch's active problems.
     if (shared) {
-      if constexpr (sizeof(T) == 4)
-        k_nufft_interp_group<T><<<dim3(interp_blocks(), interp_chunks()), 256, 0, s>>>(
-            geo, g, gstride, nx, ny, inv_mm, c.st, gate, c.part, qchi, y2, B, base, out, ippw);
+      if constexpr (sizeof(T) == 4) {
+        if (interp_fly)
+          k_nufft_interp_group_fly<T><<<dim3(interp_blocks(), interp_chunks()), 256, 0, s>>>(
+              geo, g, gstride, nx, ny, inv_mm, c.st, gate, c.part, qchi, y2, B, base, out, ippw);
+        else
+          k_nufft_interp_group<T><<<dim3(interp_blocks(), interp_chunks()), 256, 0, s>>>(
+              geo, g, gstride, nx, ny, inv_mm, c.st, gate, c.part, qchi, y2, B, base, out, ippw);
+      }
       else
         k_nufft_interp_shared<T, true><<<dim3(interp_blocks(), interp_chunks()), 256, 0, s>>>(
             geo, g, gstride, nx, ny, inv_mm, c.st, gate, c.part, qchi, y2, B, base, out, ippw);
