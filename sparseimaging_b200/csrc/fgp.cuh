@@ -73,9 +73,22 @@ __global__ void k_fgp(FgpArgs a) {
   const float* box = P.box_flag == 1 ? a.box : nullptr;
   const double* z = a.z + (size_t)b * a.xstride;
   const double* d = a.dfdx + (size_t)b * a.xstride;
-  const int nloc = nrow * NX;
   // b = xtmp (c/mfista_nufft_lib.c:424-441) ; duals start at zero
-  for (int t = threadIdx.x; t < nloc; t += blockDim.x) {
+  // thread -> (row, column) walk without integer division: rows_per_pass
+  // rows of NX columns per pass when NX <= blockDim.x, else one row with
+  // the columns strided by blockDim.x
+  const int nt = (int)blockDim.x;
+  const int rpp = NX <= nt ? nt / NX : 1;
+  const int c_step = NX <= nt ? NX : nt;
+  const int jl0 = NX <= nt ? (int)threadIdx.x / NX : 0;
+  const int ic0 = NX <= nt ? (int)threadIdx.x - jl0 * NX : (int)threadIdx.x;
+  const bool walker = jl0 < rpp;
+#define FGP_FOR_LOCAL(JL, I) \
+  if (walker)                \
+    for (int JL = jl0; JL < nrow; JL += rpp) \
+      for (int I = ic0; I < NX; I += c_step)
+  FGP_FOR_LOCAL(jl_, i_) {
+    const int t = jl_ * NX + i_;
     int f = j0 * NX + t;
     double bv;
     if (nonneg) bv = ((1.0 * (-P.lambda_l1 / c)) + d[f] * (1.0 / c)) + z[f];
@@ -120,8 +133,8 @@ __global__ void k_fgp(FgpArgs a) {
     // phase A
     {
       const T* qa = (j0 >= 1 && nrow > 0) ? peer(const_cast<T*>(qs), rank - 1) + (size_t)(rpc - 1) * NX : nullptr;
-      for (int t = threadIdx.x; t < nloc; t += blockDim.x) {
-        int jl = t / NX, i = t - jl * NX;
+      FGP_FOR_LOCAL(jl, i) {
+        const int t = jl * NX + i;
         int j = j0 + jl;
         T l = lpq(pr, qs, qa, t, i, j);
         T v = l * alpha1 + BB[t];
@@ -141,8 +154,8 @@ __global__ void k_fgp(FgpArgs a) {
     // phase B
     {
       const T* xb = (j1 < NY && nrow > 0 && rank + 1 < csize) ? peer(XV, rank + 1) : nullptr;
-      for (int t = threadIdx.x; t < nloc; t += blockDim.x) {
-        int jl = t / NX, i = t - jl * NX;
+      FGP_FOR_LOCAL(jl, i) {
+        const int t = jl * NX + i;
         int j = j0 + jl;
         T xv = XV[t];
         bool hp = i < NX - 1, hq = j < NY - 1;
@@ -181,5 +194,6 @@ __global__ void k_fgp(FgpArgs a) {
     cluster.sync();
   }
 }
+#undef FGP_FOR_LOCAL
 
 }  // namespace mf

@@ -252,9 +252,11 @@ template <typename T> struct NufftOp : Op {
   int rpc = 8, cpc = 8, tile_r = 8, tile_c = 32, ntiles = 0;
   int ippw = SharedChunk<T>::kInterpPts;  // interpolation points per warp (shared geometry)
   int spread_cs = 8;                      // spreading cluster size (shared geometry)
-  // FP32 grouped interpolation with taps formed on the fly (fewer registers)
-  // instead of held in registers; both give the same bits
-  bool interp_fly = false;
+  // FP32 grouped interpolation with taps formed on the fly (fewer registers;
+  // measured 8 % / 17 % faster with 64 / 1 problems active on the lambda
+  // grid, 7 % slower with 16) instead of held in registers; both give the
+  // same bits (MFISTA_INTERP_FLY=0 selects the register form)
+  bool interp_fly = true;
   size_t smem_rows = 0, smem_cols = 0;
   long gstride = 0;
   double inv_mm = 0;
@@ -1220,7 +1222,10 @@ struct Solver {
   template <typename T> void pick_fgp_shape() {
     int NX = ctx.tsvNX, NY = ctx.tsvNY;
     const size_t limit = 200 * 1024;
-    for (int cs : {8, 16}) {
+    // few problems: 16 CTAs per problem (more SMs busy, half the rows per CTA);
+    // otherwise 8 (the GPU is full either way, fewer cluster-wide barriers)
+    const bool few = ctx.B * 8 < 148;
+    for (int cs : {few ? 16 : 8, few ? 8 : 16}) {
       int rpc = cdiv(NY, cs);
       size_t bytes = (size_t)6 * rpc * NX * sizeof(T);
       if (bytes > limit) continue;
