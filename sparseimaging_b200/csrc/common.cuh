@@ -121,9 +121,29 @@ __device__ __forceinline__ bool gate_ok(const ProbState& s, int gate) {
 // sees the same ranking, so a problem lands in exactly one chunk however
 // the active problems are spread over the batch.  Called by all threads of
 // a 256-thread CTA; s_cnt is 8 ints of shared memory.
+//
+// Inside the device loop the ranking comes ready-made: k_select_blocks
+// writes, at the head of every step, the problems passing the three loop
+// gates in index order (`lists`: per gate slot, the count then the indices;
+// gate_list_slot), and a CTA copies its chunk from there instead of reading
+// every problem's state.  The chunks are the same either way.
+__host__ __device__ __forceinline__ int gate_list_slot(int gate) {
+  return gate == kGateGrad ? 0 : gate == kGateTrial ? 1 : gate == kGateRefresh ? 2 : -1;
+}
+constexpr int kGateLists = 3;
+
 template <int PB>
 __device__ __forceinline__ int active_chunk(const ProbState* __restrict__ st, int gate, int B, int chunk, int* list,
-                                            int* s_cnt) {
+                                            int* s_cnt, const int* __restrict__ lists = nullptr) {
+  const int gl = lists ? gate_list_slot(gate) : -1;
+  if (gl >= 0) {
+    const int* L = lists + (size_t)gl * (B + 1);
+    const int lo = chunk * PB;
+    const int cnt = min(max(L[0] - lo, 0), PB);
+    if ((int)threadIdx.x < cnt) list[threadIdx.x] = L[1 + lo + threadIdx.x];
+    __syncthreads();
+    return cnt;
+  }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int lo = chunk * PB;
   int base_rank = 0;

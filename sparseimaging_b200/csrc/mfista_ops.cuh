@@ -592,15 +592,49 @@ __global__ void k_init_state(ProbState* st, int B, int bad_nonneg_tsv) {
 // Conditional blocks of the device loop: sets the IF handles of the anchor
 // refresh block (has_ref) and of the gradient block for this step -- 1 when
 // some problem needs it -- and counts the kernels that those blocks launch
-// (launched[0]).  One CTA; the blocks' kernels keep their per-problem gates.
-__global__ void k_select_blocks(const ProbState* __restrict__ st, int B, int has_ref,
-                                cudaGraphConditionalHandle h_ref, cudaGraphConditionalHandle h_grad, int n_ref,
-                                int n_grad, unsigned long long* __restrict__ launched) {
+// (launched[0]).  With `lists` it also writes this step's problem lists of
+// the three loop gates (count, then indices in increasing order; see
+// active_chunk), which the NUFFT kernels of the step read instead of every
+// problem's state.  One CTA of 256 threads; the blocks' kernels keep their
+// per-problem gates.
+__global__ void __launch_bounds__(256) k_select_blocks(const ProbState* __restrict__ st, int B, int has_ref,
+                                                       cudaGraphConditionalHandle h_ref,
+                                                       cudaGraphConditionalHandle h_grad, int n_ref, int n_grad,
+                                                       unsigned long long* __restrict__ launched,
+                                                       int* __restrict__ lists) {
+  __shared__ int s_cnt[kGateLists][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gates[kGateLists] = {kGateGrad, kGateTrial, kGateRefresh};
+  int base[kGateLists] = {0, 0, 0};
   int g = 0, r = 0;
-  for (int b = threadIdx.x; b < B; b += blockDim.x) {
-    const ProbState& s = st[b];
-    g |= gate_ok(s, kGateGrad) ? 1 : 0;
-    r |= gate_ok(s, kGateRefresh) ? 1 : 0;
+  for (int b0 = 0; b0 < B; b0 += 256) {
+    const int b = b0 + (int)threadIdx.x;
+    bool on[kGateLists];
+#pragma unroll
+    for (int q = 0; q < kGateLists; ++q) on[q] = b < B && gate_ok(st[b], gates[q]);
+    g |= on[0] ? 1 : 0;
+    r |= on[2] ? 1 : 0;
+    if (lists) {
+      unsigned int bal[kGateLists];
+#pragma unroll
+      for (int q = 0; q < kGateLists; ++q) {
+        bal[q] = __ballot_sync(0xffffffffu, on[q]);
+        if (lane == 0) s_cnt[q][warp] = __popc(bal[q]);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < kGateLists; ++q) {
+        int rank = base[q] + __popc(bal[q] & ((1u << lane) - 1u)), tot = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+          if (w < warp) rank += s_cnt[q][w];
+          tot += s_cnt[q][w];
+        }
+        if (on[q]) lists[(size_t)q * (B + 1) + 1 + rank] = b;
+        base[q] += tot;
+      }
+      __syncthreads();  // s_cnt is rewritten by the next round
+    }
   }
   g = __syncthreads_or(g);
   r = __syncthreads_or(r);
@@ -608,6 +642,8 @@ __global__ void k_select_blocks(const ProbState* __restrict__ st, int B, int has
     if (has_ref) cudaGraphSetConditional(h_ref, r ? 1u : 0u);
     cudaGraphSetConditional(h_grad, g ? 1u : 0u);
     launched[0] += (unsigned long long)((has_ref && r ? n_ref : 0) + (g ? n_grad : 0));
+    if (lists)
+      for (int q = 0; q < kGateLists; ++q) lists[(size_t)q * (B + 1)] = base[q];
   }
 }
 

@@ -37,6 +37,7 @@ template <typename T> struct NufftGeom {
   int tile_bstride;       // ntiles, or 0 when all problems share one geometry
   long y2_bstride;        // per-problem offset of the residual, 0 if not shared
   const double* e4;       // [Nx*Ny] grid correction (shared by all problems)
+  const int* act_lists;   // this step's gate lists (device loop), or null (active_chunk)
 };
 
 // m2mr (c/mfista_nufft_lib.c:42-48)
@@ -489,7 +490,7 @@ __global__ void __launch_bounds__(256, SharedChunk<T>::kInterpMinBlocks) k_nufft
   __shared__ int s_prob[PB];  // problem of chunk slot i
   if (kActiveChunks) {
     __shared__ int s_cnt[8];
-    const int n = active_chunk<PB>(st, gate, B, blockIdx.y, s_prob, s_cnt);
+    const int n = active_chunk<PB>(st, gate, B, blockIdx.y, s_prob, s_cnt, geo.act_lists);
     if (threadIdx.x < PB) s_act[threadIdx.x] = threadIdx.x < n ? 1 : 0;
   } else if (threadIdx.x < PB) {
     const int b = blockIdx.y * PB + threadIdx.x;
@@ -710,7 +711,7 @@ __global__ void __launch_bounds__(256, GroupChunk<T>::kMinBlocks) k_nufft_interp
   __shared__ double s_chi[8][PB];  // per warp, per list slot
   __shared__ int s_list[PB];
   __shared__ int s_cnt[8];
-  const int nact = active_chunk<PB>(st, gate, B, blockIdx.y, s_list, s_cnt);
+  const int nact = active_chunk<PB>(st, gate, B, blockIdx.y, s_list, s_cnt, geo.act_lists);
   if (nact == 0) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int mtot = geo.pt_hi[0];
@@ -893,7 +894,7 @@ __global__ void __launch_bounds__(256, 3) k_nufft_interp_group_fly(
   __shared__ int s_list[PB];
   __shared__ int s_cnt[8];
   __shared__ T s_wt[8][2][kTaps];  // per warp: the point's wx, wy
-  const int nact = active_chunk<PB>(st, gate, B, blockIdx.y, s_list, s_cnt);
+  const int nact = active_chunk<PB>(st, gate, B, blockIdx.y, s_list, s_cnt, geo.act_lists);
   if (nact == 0) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int mtot = geo.pt_hi[0];
@@ -1130,7 +1131,7 @@ __global__ void __launch_bounds__(256, SharedChunk<T>::kSpreadMinBlocks) k_nufft
   const int csize = (int)cluster.num_blocks();
   // chunks over the batch's active problems (list: problem indices)
   __shared__ int s_cnt[8];
-  const int cnt = active_chunk<PB>(st, gate, B, blockIdx.y, sm.list, s_cnt);
+  const int cnt = active_chunk<PB>(st, gate, B, blockIdx.y, sm.list, s_cnt, geo.act_lists);
   if (cnt == 0) return;  // uniform over the cluster: same problem chunk
   const int b0 = 0;
   // densest tiles first, so that the longest clusters start in the first wave

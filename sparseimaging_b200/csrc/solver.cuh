@@ -133,6 +133,9 @@ struct Ctx {
   ProbParams* prm = nullptr;
   ProbState* st = nullptr;
   Partials part{};
+  // per-step gate lists (k_select_blocks), given to the kernels captured in
+  // the device loop's body; null everywhere else
+  const int* act_lists = nullptr;
 };
 
 // Launch shapes of the operator kernels that the autotuner may change.
@@ -392,8 +395,16 @@ template <typename T> struct NufftOp : Op {
   static size_t spread_smem() { return sizeof(cplx<T>) * SharedChunk<T>::kSpread * 256; }
   int spread_chunks() const { return cdiv(B, SharedChunk<T>::kSpread); }
 
+  // the geometry with this launch's gate lists (set inside the device loop)
+  NufftGeom<T> geo_now() const {
+    NufftGeom<T> g = geo;
+    g.act_lists = c.act_lists;
+    return g;
+  }
+
   void launch_interp(cudaStream_t s, cplx<T>* g, int gate, int qchi, cplx<T>* y2, const double2* base = nullptr,
                      double2* out = nullptr) {
+    const NufftGeom<T> geo = geo_now();
     // FP32: grouped kernel; FP64 (register-bound with 2G double sums): one
     // problem at a time.  Both chunk the batch's active problems.
     if (shared) {
@@ -475,6 +486,7 @@ template <typename T> struct NufftOp : Op {
   }
 
   void launch_spread(cudaStream_t s, cplx<T>* g, int gate) {
+    const NufftGeom<T> geo = geo_now();
     if (shared) {
       // cluster of spread_cs CTAs per tile, each a segment of its points
       cudaLaunchConfig_t cfg = {};
@@ -1070,7 +1082,7 @@ struct Solver {
   int fgp_iter = 100;
   int refresh_every = 0;  // defect correction: anchor refresh period (outer iterations)
   int step_cap = 0;
-  DevMem d_x, d_z, d_xnew, d_dfdx, d_xa, d_prm, d_st, d_part, d_out, d_box, d_fgp, d_steps, d_ticket;
+  DevMem d_x, d_z, d_xnew, d_dfdx, d_xa, d_prm, d_st, d_part, d_out, d_box, d_fgp, d_steps, d_ticket, d_lists;
   unsigned long long step_budget = 0;
   ImgDims dm{};
   cudaStream_t stream = nullptr, cap_stream = nullptr, cap_block = nullptr;
@@ -1143,6 +1155,8 @@ struct Solver {
     d_steps.alloc(3 * sizeof(unsigned long long));
     d_ticket.alloc(sizeof(unsigned int));
     MF_CK(cudaMemset(d_ticket.p, 0, sizeof(unsigned int)));
+    d_lists.alloc(sizeof(int) * (size_t)kGateLists * (B + 1));
+    MF_CK(cudaMemset(d_lists.p, 0, d_lists.bytes));
     ctx.x = d_x.as<double>();
     ctx.z = d_z.as<double>();
     ctx.xnew = d_xnew.as<double>();
@@ -1363,8 +1377,10 @@ struct Solver {
       if (op->corrected()) MF_CK(cudaGraphConditionalHandleCreate(&h_ref, g, 0, 0));
       MF_CK(cudaGraphConditionalHandleCreate(&h_grad, g, 0, 0));
       k_select_blocks<<<1, 256, 0, s>>>(ctx.st, ctx.B, op->corrected() ? 1 : 0, h_ref, h_grad, ref_block_launches,
-                                        grad_block_launches, d_steps.as<unsigned long long>() + 2);
+                                        grad_block_launches, d_steps.as<unsigned long long>() + 2,
+                                        d_lists.as<int>());
       MF_LAUNCH_CK();
+      ctx.act_lists = d_lists.as<int>();  // for the NUFFT kernels of this step
     }
     if (op->corrected()) {  // new FP64 anchor x_a = x every refresh_every outer iterations
       cudaStream_t bs = cond ? begin_if(s, h_ref) : s;
@@ -1407,6 +1423,7 @@ struct Solver {
     k_momentum<<<dim3(img_blocks() + op->model_blocks(), ctx.B), 256, 0, s>>>(ctx.x, ctx.z, ctx.xnew, dm, ctx.st,
                                                                             op->model_momentum(img_blocks()));
     MF_LAUNCH_CK();
+    ctx.act_lists = nullptr;
   }
 
   void drop_graphs() {
@@ -1507,6 +1524,7 @@ struct Solver {
     cond_blocks = false;
     if (!host_loop) {
       cudaError_t e = try_build_conditional();
+      ctx.act_lists = nullptr;  // only the captured loop body uses them
       if (e == cudaSuccess) return;
       cudaGetLastError();
       if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
