@@ -436,6 +436,7 @@ __global__ void __launch_bounds__(kControlThreads) k_control(const ProbParams* _
                                                  int* __restrict__ any_active, unsigned int* __restrict__ ticket) {
   __shared__ double red[kNumQ];
   __shared__ int s_skip;
+  __shared__ int s_last;
   const int b = blockIdx.x;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) s_skip = (cfg.mode == kCtrlStep && !st[b].active) ? 1 : 0;
@@ -563,11 +564,16 @@ __global__ void __launch_bounds__(kControlThreads) k_control(const ProbParams* _
     }
     st[b] = s;
     __threadfence();
-    unsigned int t = atomicAdd(ticket, 1u);
-    if (t == gridDim.x - 1) {  // last problem done: publish the loop condition
-      __threadfence();
-      int any = 0;
-      for (int k = 0; k < gridDim.x; ++k) any |= ((volatile ProbState*)st)[k].active;
+    s_last = atomicAdd(ticket, 1u) == gridDim.x - 1 ? 1 : 0;
+  }
+  __syncthreads();
+  if (s_last) {  // last problem done: publish the loop condition
+    __threadfence();
+    // the whole CTA reads the problems' flags
+    int any = 0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) any |= ((volatile ProbState*)st)[k].active;
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) {
       if (set_handle) cudaGraphSetConditional(handle, any ? 1u : 0u);
       if (any_active) *any_active = any;
       if (cfg.mode == kCtrlStep && cfg.steps) cfg.steps[0] += 1ull;
