@@ -31,6 +31,7 @@ from . import lib as _lib_loader
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "data", "unet_warmstart_128.npy")
+WEIGHTS_256 = os.path.join(HERE, "data", "unet_warmstart_256.npy")  # config 4 (config4_main)
 TRAIN_LAMBDA = 1e-3  # training targets: lambda_l1 = lambda_tsv = 1e-3 max|A^H W^2 y|
 
 _bound = False
@@ -166,10 +167,11 @@ def choose_starts(geo, problems, x_warm, precision=None):
     return starts, used
 
 
-def load(nx=128, batch_max=8, path=WEIGHTS):
-    """The trained network (raises if the weights file is absent)."""
+def load(nx=128, batch_max=8, path=None):
+    """The trained network (raises if the weights file is absent): the
+    128 x 128 lambda-grid weights, or for nx = 256 the config-4 weights."""
     net = UNet(nx, nx, batch_max)
-    net.set_params(np.load(path))
+    net.set_params(np.load(path or (WEIGHTS_256 if nx == 256 else WEIGHTS)))
     return net
 
 
@@ -391,7 +393,7 @@ def main():
     a = ap.parse_args()
     os.environ.setdefault("MFISTA_QUIET", "1")
     if a.config4:
-        out = a.out if a.out != WEIGHTS else os.path.join(HERE, "data", "unet_warmstart_256.npy")
+        out = a.out if a.out != WEIGHTS else WEIGHTS_256
         config4_main(a.n_train, a.n_eval, a.steps, out, a.json)
         return
     if not a.train:
