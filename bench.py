@@ -18,7 +18,9 @@ figure repeats the chosen solve through mfista_nufft_batch from pinned host
 arrays.  Side measurements (untimed for `value`): the DFT lambda grid in
 FP64 and the tensor-core split-BF16 forms, the leave-one-out error of its
 solutions against a numpy/LAPACK host baseline, a 48-frame movie batch and
-the same frames solved as one movie with the temporal term.
+the same frames solved as one movie with the temporal term, the FFT variant
+with TV / FGP 50 in FP64 and FP32 (with the FGP kernel's rate), and the
+learned warm start at 256 x 256 on held-out skies.
 Multi-GPU: every rank solves its own seeded lambda grid (no collective on
 the data path), value = all ranks' solves / max-over-ranks time (weak
 scaling).
@@ -256,6 +258,26 @@ def fft_config1(si, hbm_gbs):
     out["fgp_kernel"] = fgp
     out["fgp_kernel_note"] = ("k_fgp: 50 FGP iterations of one prox per problem inside one launch (slabs in shared "
                               "memory, DSMEM halos); compulsory bytes 24 B/pixel per prox (z, dfdx in, xnew out)")
+    return out
+
+
+def warmstart_config4(si, n=32):
+    """Side measurement of the learned warm start at the config-4 scale
+    (256 x 256, M = 19998 shared coverage; sparseimaging_b200/data/
+    unet_warmstart_256.npy, trained on 1024 FP64-solved skies): n held-out
+    skies solved by FP64 MFISTA to F*(1 + 1e-6) from zero and from the
+    network's start; iterations, solves/s (the network's prediction and the
+    choice of start included) and image error against x* (4000 FP64
+    iterations)."""
+    from sparseimaging_b200 import warmstart
+    net = warmstart.load(256)
+    try:
+        ev = warmstart.evaluate(net, list(range(90000, 90000 + n)), nx=256, batch=n, fstar_iters=4000)
+    finally:
+        net.close()
+    out = {"workload": f"256x256, M = 19998 (12 stations x 303 hour angles), {n} held-out skies, "
+                       "lambda_l1 = lambda_tsv = 1e-3 max|A^H W^2 y|"}
+    out.update(ev["summary"])
     return out
 
 
@@ -602,7 +624,8 @@ def run_ours(args):
     side = {}
     if rank == 0:  # side measurements of the other configurations (rank 0 only)
         for key, fn in (("dft_lambda_grid", dft_lambda_grid), ("movie_batch", movie_batch),
-                        ("fft_tv_fgp50", lambda s_: fft_config1(s_, hbm))):
+                        ("fft_tv_fgp50", lambda s_: fft_config1(s_, hbm)),
+                        ("warmstart_config4", warmstart_config4)):
             try:
                 side[key] = fn(si)
             except Exception as e:  # reported, not required
