@@ -145,7 +145,9 @@ struct mfista_problem {
  * the GPU, each with its own backtracking state and convergence mask.
  *   geometry: if shared_geometry != 0 all problems use the M points of
  *     u_dx/v_dy/vis_*; otherwise problem b uses points
- *     [pt_off[b], pt_off[b+1]) of the concatenated arrays (uneven M).
+ *     [pt_off[b], pt_off[b+1]) of the concatenated arrays (uneven M), and
+ *     M is their length, or 0 to take it as pt_off[B]; pt_off must start
+ *     at >= 0, never decrease and end at <= M (else MFISTA_ERR_ARG).
  *   eps is scaled per problem exactly as mfista_imaging_core_nufft does.
  *   xinit: [B*Nx*Ny] or NULL (zero start); xout: [B*Nx*Ny];
  *   results: [B] RESULT records (residual left NULL).

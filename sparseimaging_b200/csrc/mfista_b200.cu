@@ -278,6 +278,8 @@ extern "C" mfista_plan mfista_nufft_plan_create(const double* u_dx, const double
       if (pt_off[0] < 0) throw Error(MFISTA_ERR_ARG, "pt_off[0] must be >= 0");
       for (int b = 0; b < B; ++b)
         if (pt_off[b + 1] < pt_off[b]) throw Error(MFISTA_ERR_ARG, "pt_off must not decrease");
+      // M > 0 is the length of the concatenated point arrays
+      if (M > 0 && pt_off[B] > M) throw Error(MFISTA_ERR_ARG, "pt_off[B] exceeds M, the length of the point arrays");
     }
     std::unique_ptr<mfista_plan_s> P(new mfista_plan_s);
     P->B = B;

@@ -156,3 +156,22 @@ def test_device_loop_matches_host_loop(gpulib, c0, precision, monkeypatch):
     assert [r["finalcost"] for r in Rd] == [r["finalcost"] for r in Rh]
     if precision == "fp32":
         assert Ld < Lh
+
+
+def test_batch_rejects_offsets_beyond_the_arrays(gpulib, c0):
+    """Independent geometry: pt_off[B] larger than M (the length of the
+    concatenated point arrays) is rejected before anything reads them."""
+    import ctypes as C
+    m = 100
+    u = np.ascontiguousarray(c0["u"][:m])
+    arrs = [np.ascontiguousarray(c0[k][:m], np.float64) for k in ("u", "v", "vis_r", "vis_i", "vis_std")]
+    off = np.array([0, 50, 150], np.int32)
+    probs = gpulib._problems(_problems(c0, [1.0, 1.0], 10))
+    xo = np.zeros(2 * 64 * 64)
+    res = (gpulib.RESULT * 2)()
+    dp = C.POINTER(C.c_double)
+    st = gpulib.lib().mfista_nufft_batch(*[a.ctypes.data_as(dp) for a in arrs], off.ctypes.data_as(C.POINTER(C.c_int)),
+                                         0, m, 64, 64, 2, probs, 1e-5, gpulib.FP64, 100, None,
+                                         xo.ctypes.data_as(dp), res)
+    assert st == 2
+    assert u.size == m
