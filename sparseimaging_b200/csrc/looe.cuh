@@ -51,18 +51,14 @@ __global__ void __launch_bounds__(256) k_looe_gemm(int m, int n, int k, double a
   __shared__ double As[kGK][kGT + 1];
   __shared__ double Bs[kGK][kGT + 1];
   const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
-  constexpr int kLd = (kGT * kGK) / 256;  // elements of each operand a thread stages per k step
   double acc[4][4];
 #pragma unroll
   for (int r = 0; r < 4; ++r)
 #pragma unroll
     for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
-  // the next k step's tile elements are loaded into registers while the
-  // current one is multiplied out of shared memory (register double buffer)
-  double ra[kLd], rb[kLd];
-  auto fetch = [&](int p0) {
+  for (int p0 = 0; p0 < k; p0 += kGK) {
 #pragma unroll
-    for (int q = 0; q < kLd; ++q) {
+    for (int q = 0; q < (kGT * kGK) / 256; ++q) {
       const int e = t + 256 * q;
       int i, p;
       if (TA) {
@@ -73,7 +69,9 @@ __global__ void __launch_bounds__(256) k_looe_gemm(int m, int n, int k, double a
         p = e / kGT;
       }
       const int gi = i0 + i, gp = p0 + p;
-      ra[q] = (gi < m && gp < k) ? (TA ? A[(size_t)gp + (size_t)gi * lda] : A[(size_t)gi + (size_t)gp * lda]) : 0.0;
+      double v = 0.0;
+      if (gi < m && gp < k) v = TA ? A[(size_t)gp + (size_t)gi * lda] : A[(size_t)gi + (size_t)gp * lda];
+      As[p][i] = v;
       int j;
       if (TB) {
         j = e % kGT;
@@ -83,24 +81,11 @@ __global__ void __launch_bounds__(256) k_looe_gemm(int m, int n, int k, double a
         p = e % kGK;
       }
       const int gj = j0 + j, gq = p0 + p;
-      rb[q] = (gj < n && gq < k) ? (TB ? B[(size_t)gj + (size_t)gq * ldb] : B[(size_t)gq + (size_t)gj * ldb]) : 0.0;
+      double w = 0.0;
+      if (gj < n && gq < k) w = TB ? B[(size_t)gj + (size_t)gq * ldb] : B[(size_t)gq + (size_t)gj * ldb];
+      Bs[p][j] = w;
     }
-  };
-  auto stash = [&]() {
-#pragma unroll
-    for (int q = 0; q < kLd; ++q) {
-      const int e = t + 256 * q;
-      if (TA) As[e % kGK][e / kGK] = ra[q];
-      else As[e / kGT][e % kGT] = ra[q];
-      if (TB) Bs[e / kGT][e % kGT] = rb[q];
-      else Bs[e % kGK][e / kGK] = rb[q];
-    }
-  };
-  if (k > 0) fetch(0);
-  for (int p0 = 0; p0 < k; p0 += kGK) {
-    stash();
     __syncthreads();
-    if (p0 + kGK < k) fetch(p0 + kGK);
 #pragma unroll
     for (int p = 0; p < kGK; ++p) {
       double a[4], b[4];

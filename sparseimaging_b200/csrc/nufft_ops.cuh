@@ -458,7 +458,7 @@ template <> struct SharedChunk<float> {
   static constexpr int kInterp = 16;  // problems per interpolation CTA
   static constexpr int kSpread = 16;  // problems per spreading CTA
   static constexpr int kInterpMinBlocks = 3;
-  static constexpr int kInterpPts = 2;  // default points per warp
+  static constexpr int kInterpPts = 1;  // default points per warp (what the autotuner picks on the lambda grid)
   static constexpr int kSpreadMinBlocks = 3;
 };
 template <> struct SharedChunk<double> {

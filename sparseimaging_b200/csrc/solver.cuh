@@ -252,7 +252,9 @@ template <typename T> struct NufftOp : Op {
   DevMem d_tord;  // shared geometry: spreading tiles by falling point count
   FftHost<T> fh, fcol;
   NufftGeom<T> geo{};
-  int rpc = 8, cpc = 8, tile_r = 8, tile_c = 32, ntiles = 0;
+  // default launch shapes: the autotuner's choice on the 128 x 128 lambda
+  // grid (FP32: 4 columns per CTA)
+  int rpc = 8, cpc = sizeof(T) == 4 ? 4 : 8, tile_r = 8, tile_c = 32, ntiles = 0;
   int ippw = SharedChunk<T>::kInterpPts;  // interpolation points per warp (shared geometry)
   int spread_cs = 8;                      // spreading cluster size (shared geometry)
   // FP32 grouped interpolation with taps formed on the fly (fewer registers;
