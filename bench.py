@@ -198,21 +198,30 @@ def _reported(fn, *args):
 
 
 def movie_joint(si, geo, off, probs):
-    """The same 48 frames solved as ONE movie (mfista_nufft_movie, FP64):
-    one lambda (the frames' median), temporal weight lambda_t = 5 lambda
-    and 0 (uncoupled frames under one step size), 1000 iterations each;
-    time per solve and the temporal term sum_b |x_b - x_{b+1}|^2 it
-    leaves."""
+    """The same 48 frames solved as ONE movie (mfista_nufft_movie): one
+    lambda (the frames' median), temporal weight lambda_t = 5 lambda in the
+    FP64 and the FP32 form, and 0 (uncoupled frames under one step size),
+    1000 iterations each; time per solve, the temporal term
+    sum_b |x_b - x_{b+1}|^2 it leaves, the objective, and the FP32 form's
+    objective and images against the FP64 form's."""
     lam = float(np.median([q["lambda_l1"] for q in probs]))
     lip = float(max(q["cinit"] for q in probs))
     out = {"frames": len(probs), "iterations": 1000, "lambda_t_over_lambda": 5.0}
-    for name, lt in (("coupled", 5.0 * lam), ("uncoupled", 0.0)):
-        X, R, tcost = si.nufft_movie(*geo[:5], off, geo[5], geo[6], lam, 1e-3 * lam, lt, lip, 1000, 0.0)
+    imgs = {}
+    for name, lt, prec in (("coupled", 5.0 * lam, si.FP64), ("coupled_fp32", 5.0 * lam, si.FP32),
+                           ("uncoupled", 0.0, si.FP64)):
+        X, R, tcost = si.nufft_movie(*geo[:5], off, geo[5], geo[6], lam, 1e-3 * lam, lt, lip, 1000, 0.0,
+                                     precision=prec)
         D = X[:-1] - X[1:]
+        imgs[name] = X
         out[name] = {"solve_s": round(R[0]["comp_time"], 4),
                      "iterations_per_s": round(R[0]["ITER"] / R[0]["comp_time"], 1),
                      "temporal_sum": float(np.sum(D * D)),
                      "objective": float(sum(r["finalcost"] for r in R) + tcost)}
+    a, b = out["coupled_fp32"]["objective"], out["coupled"]["objective"]
+    out["coupled_fp32"]["rel_objective_vs_fp64"] = abs(a - b) / b
+    out["coupled_fp32"]["rel_image_vs_fp64"] = float(np.linalg.norm(imgs["coupled_fp32"] - imgs["coupled"]) /
+                                                     np.linalg.norm(imgs["coupled"]))
     return out
 
 

@@ -172,13 +172,20 @@ int mfista_nufft_batch(const double *u_dx, const double *v_dy, const double *vis
  * xout: [n_frames*Nx*Ny]; results: [n_frames] per-frame terms (finalcost
  * without the temporal term; ITER and Lip_const are the joint ones);
  * temporal_cost: lambda_t times the temporal sum at xout (may be NULL).
- * FP64, TSV form (the matlab code has no TV form), no box constraint.
+ * c_box: [Nx*Ny] pixel weights or NULL: the starting image is xinit .* c_box
+ * and every thresholded image is multiplied by c_box pixel by pixel, as the
+ * matlab code's c_box (MFISTA_movie_eht.m:46, :143-146; a 0/1 mask is a
+ * support constraint).
+ * precision: MFISTA_FP64, or MFISTA_FP32 (FP32 NUFFTs with the FP64 anchor
+ * correction of mfista_nufft_batch; objective, backtracking and momentum in
+ * FP64).  TSV form (the matlab code has no TV form).
  * No counterpart in the reference's C library. */
 int mfista_nufft_movie(const double *u_dx, const double *v_dy, const double *vis_r, const double *vis_i,
                        const double *vis_std, const int *pt_off, int n_frames, int Nx, int Ny,
                        const double *t_list, double lambda_l1, double lambda_tsv, double lambda_t,
-                       double cinit, int maxiter, double eps, int nonneg_flag, const double *xinit,
-                       double *xout, struct RESULT *results, double *temporal_cost);
+                       double cinit, int maxiter, double eps, int nonneg_flag, const double *c_box,
+                       int precision, const double *xinit, double *xout, struct RESULT *results,
+                       double *temporal_cost);
 
 /* Batched DFT solve (B problems sharing the column-major M x N matrix A and
  * the data y, e.g. a lambda grid): A z and A^T r run as GEMMs over the

@@ -48,9 +48,11 @@ def dt_x(X, wt):
     return G
 
 
-def movie(frames, nx, ny, lam, lam2, lam_t, cinit, maxiter, eps, nonneg_flag=1, t_list=None, xinit=None):
-    """frames: list of (u, v, vis_r, vis_i, vis_std).  Returns (X [T][N],
-    iterations, c, cost history)."""
+def movie(frames, nx, ny, lam, lam2, lam_t, cinit, maxiter, eps, nonneg_flag=1, t_list=None, xinit=None,
+          c_box=None):
+    """frames: list of (u, v, vis_r, vis_i, vis_std).  c_box: [N] pixel
+    weights or None (x = xinit .* c_box, :46; every thresholded image times
+    c_box, :143-146).  Returns (X [T][N], iterations, c, cost history)."""
     T = len(frames)
     N = nx * ny
     t = np.arange(1, T + 1, dtype=np.float64) if t_list is None else np.asarray(t_list, np.float64)
@@ -60,7 +62,12 @@ def movie(frames, nx, ny, lam, lam2, lam_t, cinit, maxiter, eps, nonneg_flag=1, 
         plan = NufftPlan(u, v, nx, ny)
         w = 1.0 / np.asarray(vs, np.float64)
         ops.append((plan, np.asarray(vr, np.float64), np.asarray(vi, np.float64), w))
-    prox = soft_threshold_nonneg if nonneg_flag == 1 else soft_threshold
+    soft = soft_threshold_nonneg if nonneg_flag == 1 else soft_threshold
+    box = None if c_box is None else np.asarray(c_box, np.float64)
+
+    def prox(v, eta):
+        out = soft(v, eta)
+        return out if box is None else out * box[None, :]
 
     def frame_costs(X):
         """sum_b chi2_b/2 + lam2 TSV(x_b), and the residuals."""
@@ -72,6 +79,8 @@ def movie(frames, nx, ny, lam, lam2, lam_t, cinit, maxiter, eps, nonneg_flag=1, 
         return tot, res
 
     x0 = np.zeros(N) if xinit is None else np.asarray(xinit, np.float64)
+    if box is not None:
+        x0 = x0 * box
     X = np.tile(x0, (T, 1))
     Z = X.copy()
     c, mu = float(cinit), 1.0

@@ -140,7 +140,7 @@ def lib():
         L.mfista_nufft_movie.restype = C.c_int
         L.mfista_nufft_movie.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, C.c_int, C.c_int, C.c_int, _dp, C.c_double,
                                          C.c_double, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int, _dp,
-                                         _dp, C.POINTER(RESULT), _dp]
+                                         C.c_int, _dp, _dp, C.POINTER(RESULT), _dp]
         L.mfista_cpp_y2x_nufft.restype = C.c_int
         L.mfista_cpp_y2x_nufft.argtypes = [_dp, _dp, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]
         L.mfista_cpp_imaging_core_nufft.restype = None
@@ -407,11 +407,13 @@ def dft_profile(A, B, kernel, precision=None, reps=20):
 
 
 def nufft_movie(u_dx, v_dy, vis_r, vis_i, vis_std, pt_off, nx, ny, lambda_l1, lambda_tsv, lambda_t, cinit,
-                maxiter, eps, nonneg_flag=1, t_list=None, xinit=None):
+                maxiter, eps, nonneg_flag=1, t_list=None, xinit=None, c_box=None, precision=FP64):
     """Movie of len(pt_off) - 1 frames solved as one problem with the
     temporal term lambda_t sum_b |x_b - x_{b+1}|^2 / (t_{b+1} - t_b)
-    (mfista_nufft_movie).  Returns (X [T][nx*ny], per-frame RESULT dicts,
-    temporal cost at X)."""
+    (mfista_nufft_movie).  c_box: [nx*ny] pixel weights applied to the
+    starting image and to every thresholded image (the matlab code's c_box).
+    precision: FP64 or FP32 (corrected FP32 NUFFTs).  Returns (X [T][nx*ny],
+    per-frame RESULT dicts, temporal cost at X)."""
     u, v, vr, vi, vs = (_d(a) for a in (u_dx, v_dy, vis_r, vis_i, vis_std))
     off = np.ascontiguousarray(pt_off, np.int32)
     T = off.size - 1
@@ -420,9 +422,12 @@ def nufft_movie(u_dx, v_dy, vis_r, vis_i, vis_std, pt_off, nx, ny, lambda_l1, la
     tc = C.c_double(0)
     tl = None if t_list is None else _d(t_list)
     xi = None if xinit is None else _d(xinit)
+    cb = None if c_box is None else _d(c_box)
+    if cb is not None and cb.size != nx * ny:
+        raise ValueError("c_box needs nx * ny values")
     _check(lib().mfista_nufft_movie(_p(u), _p(v), _p(vr), _p(vi), _p(vs), off.ctypes.data_as(_ip), T, nx, ny,
                                     _p(tl), lambda_l1, lambda_tsv, lambda_t, cinit, maxiter, eps, nonneg_flag,
-                                    _p(xi), _p(xo), res, C.byref(tc)))
+                                    _p(cb), precision, _p(xi), _p(xo), res, C.byref(tc)))
     return xo.reshape(T, nx * ny), [r.as_dict() for r in res], tc.value
 
 

@@ -883,8 +883,9 @@ extern "C" int mfista_dft_looe(const double* y, const double* A, int M, int N, i
 extern "C" int mfista_nufft_movie(const double* u_dx, const double* v_dy, const double* vis_r, const double* vis_i,
                                   const double* vis_std, const int* pt_off, int n_frames, int Nx, int Ny,
                                   const double* t_list, double lambda_l1, double lambda_tsv, double lambda_t,
-                                  double cinit, int maxiter, double eps, int nonneg_flag, const double* xinit,
-                                  double* xout, struct RESULT* results, double* temporal_cost) {
+                                  double cinit, int maxiter, double eps, int nonneg_flag, const double* c_box,
+                                  int precision, const double* xinit, double* xout, struct RESULT* results,
+                                  double* temporal_cost) {
   set_ok();
   try {
     if (n_frames < 1 || Nx < 1 || Ny < 1) throw Error(MFISTA_ERR_ARG, "mfista_nufft_movie: bad sizes");
@@ -893,6 +894,8 @@ extern "C" int mfista_nufft_movie(const double* u_dx, const double* v_dy, const 
     if (maxiter < 0) throw Error(MFISTA_ERR_ARG, "maxiter must be >= 0");
     if (nonneg_flag != 0 && nonneg_flag != 1) throw Error(MFISTA_ERR_ARG, "nonneg_flag must be 0 or 1");
     if (lambda_t < 0 || lambda_tsv < 0) throw Error(MFISTA_ERR_ARG, "lambda_t and lambda_tsv must be >= 0");
+    if (precision != MFISTA_FP64 && precision != MFISTA_FP32)
+      throw Error(MFISTA_ERR_ARG, "mfista_nufft_movie: precision must be MFISTA_FP64 or MFISTA_FP32");
     if (pt_off[0] < 0) throw Error(MFISTA_ERR_ARG, "pt_off[0] must be >= 0");
     for (int b = 0; b < n_frames; ++b)
       if (pt_off[b + 1] < pt_off[b]) throw Error(MFISTA_ERR_ARG, "pt_off must not decrease");
@@ -904,19 +907,22 @@ extern "C" int mfista_nufft_movie(const double* u_dx, const double* v_dy, const 
     }
     const int N = Nx * Ny;
     Solver S;
-    S.precision = MFISTA_FP64;
+    S.precision = precision;
     S.init_common(n_frames, N, Nx, Ny, kFormTSV, 100, nullptr);
     NufftInput in{u_dx, v_dy, vis_r, vis_i, vis_std, pt_off, 0, 0, Nx, Ny};
-    S.op.reset(new NufftOp<double>(S.ctx, in));
+    if (precision == MFISTA_FP32) S.op.reset(new NufftOp<float>(S.ctx, in, true));
+    else S.op.reset(new NufftOp<double>(S.ctx, in));
     S.set_movie(wt, lambda_t);
+    if (c_box) S.set_mask(c_box);
     S.finish_setup();
     std::vector<ProbParams> prm(n_frames);
     for (int b = 0; b < n_frames; ++b)
       prm[b] = ProbParams{lambda_l1, 0.0, lambda_tsv, cinit, eps, maxiter, nonneg_flag, 0, 0, 0.0};
     std::vector<double> x0;
-    if (xinit) {
+    if (xinit) {  // x = (xinit .* c_box) for every frame (MFISTA_movie_eht.m:46)
       x0.resize((size_t)n_frames * N);
-      for (int b = 0; b < n_frames; ++b) std::copy(xinit, xinit + N, x0.begin() + (size_t)b * N);
+      for (int b = 0; b < n_frames; ++b)
+        for (int f = 0; f < N; ++f) x0[(size_t)b * N + f] = c_box ? xinit[f] * c_box[f] : xinit[f];
     }
     double t0 = now_s();
     S.upload_problems(prm, xinit ? x0.data() : nullptr);

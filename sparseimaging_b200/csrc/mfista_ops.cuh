@@ -78,7 +78,8 @@ struct ImgDims {
 // ---------------------------------------------------------------------------
 __global__ void k_update_tsv(const double* __restrict__ zall, const double* __restrict__ dall,
                              double* __restrict__ xnall, ImgDims dm, const ProbParams* __restrict__ prm,
-                             const ProbState* __restrict__ st, const float* __restrict__ box, Partials part) {
+                             const ProbState* __restrict__ st, const float* __restrict__ box,
+                             const double* __restrict__ mask, Partials part) {
   __shared__ double sh[5 * 32];
   int b = blockIdx.y;
   if (!gate_ok(st[b], kGateTrial)) return;
@@ -90,10 +91,16 @@ __global__ void k_update_tsv(const double* __restrict__ zall, const double* __re
   const double* d = dall + (size_t)b * dm.xstride;
   double* xn = xnall + (size_t)b * dm.xstride;
   const float* bx = p.box_flag == 1 ? box : nullptr;
+  // the movie's c_box (matlab/MFISTA_movie_eht.m:143-146) scales the
+  // thresholded image pixel by pixel
+  auto prox_at = [&](int ff) {
+    const double pv = prox_l1(d[ff] * cinv + z[ff], eta, p.nonneg, bx, ff);
+    return mask ? pv * mask[ff] : pv;
+  };
   double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f < dm.N) {
-    double xv = prox_l1(d[f] * cinv + z[f], eta, p.nonneg, bx, f);
+    double xv = prox_at(f);
     xn[f] = xv;
     double df = xv - z[f];
     v[0] = d[f] * df;
@@ -102,11 +109,11 @@ __global__ void k_update_tsv(const double* __restrict__ zall, const double* __re
     if (p.lambda_tsv > 0) {
       int i = f % dm.NX, j = f / dm.NX;
       if (i < dm.NX - 1) {
-        double o = prox_l1(d[f + 1] * cinv + z[f + 1], eta, p.nonneg, bx, f + 1);
+        double o = prox_at(f + 1);
         v[3] += (xv - o) * (xv - o);
       }
       if (j < dm.NY - 1) {
-        double o = prox_l1(d[f + dm.NX] * cinv + z[f + dm.NX], eta, p.nonneg, bx, f + dm.NX);
+        double o = prox_at(f + dm.NX);
         v[3] += (xv - o) * (xv - o);
       }
       v[4] = tsv_pairs_at(z, f, dm.NX, dm.NY);
@@ -376,7 +383,7 @@ __device__ void control_joint(const ProbParams* __restrict__ prm, ProbState* __r
       s.active = 0;
       s.iters_out = s.iter + 1;
     } else {
-      bool finish = fval <= qval;
+      bool finish = fval <= qval + cfg.bt_slack * fabs(qval);
       if (!finish) {
         s.c *= kEta;
         s.trial += 1;
@@ -412,6 +419,7 @@ __device__ void control_joint(const ProbParams* __restrict__ prm, ProbState* __r
             s.iters_out = p.maxiter;
           } else {
             s.need_grad = 1;
+            s.refresh = (cfg.refresh_every > 0 && s.iter % cfg.refresh_every == 0) ? 1 : 0;
           }
         }
       }

@@ -952,6 +952,283 @@ __global__ void __launch_bounds__(256, 3) k_nufft_interp_group_fly(
   }
 }
 
+// ---------------------------------------------------------------------------
+// Interpolation on the tensor cores (FP32 form, shared geometry)
+//
+// Every problem's grid is one matrix G (cells x problems), and interpolation
+// is y = S G with S the points' tap weights.  The points are binned by their
+// first tap (mx - 11, my - 11) into 8 x 8 tiles of the *virtual* grid (rows
+// and columns before the wrap and the Hermitian fold), so a tile's points
+// read a 32 x 32 window of virtual cells (31 used).  A CTA takes up to 128
+// points of one tile and a chunk of 8 problems: it stages the window once in
+// shared memory, every cell already resolved to its stored cell (direct, or
+// mirrored with the conjugate) and to the sign the reference gives the
+// imaginary part there (NU_SIGN on direct taps), so all points then run the
+// same tap arithmetic with no per-tap tests.  The weights are separable,
+// S[p, (r, c)] = wx_p[r] wy_p[c], so for each window row r a warp forms
+// T_r = Wy G_r (16 points x 32 columns times 32 columns x 16 problem
+// columns) with mma.sync m16n8k8 TF32 and adds wx_p[r] T_r to its result.
+// Both operands are split into two TF32 parts (x = hi + lo) and the product
+// taken as lo*hi + hi*lo + hi*hi with FP32 accumulation (about 2^-21
+// relative per product, the accuracy of FP32 sums over the 576 taps).  The
+// epilogue is the one of k_nufft_interp_group: FP64 residual, chi^2, the
+// models of the corrected form.
+// ---------------------------------------------------------------------------
+constexpr int kItcTile = 8;    // home tile (first-tap positions per axis)
+constexpr int kItcWin = 32;    // window cells per axis
+constexpr int kItcProb = 8;    // problems per CTA (16 real columns)
+constexpr int kItcPts = 128;   // points per CTA: 8 warps x 16
+struct ItcTile {
+  int row0, col0;    // window origin in virtual cells
+  int start, count;  // this CTA's points: perm[start, start + count)
+};
+// perm entries: point index (24 bits) | first-tap row - row0 (3 bits) << 24
+// | first-tap column - col0 (3 bits) << 27
+constexpr int kItcMaxPoints = 1 << 24;
+constexpr size_t kItcSmem =
+    sizeof(float) * ((size_t)kItcWin * kItcWin * 2 * kItcProb + 8 * 16 * 36 + 8 * kItcWin * 17);
+
+// x = hi + lo: hi is x rounded to the TF32 grid (half-ulp up in magnitude,
+// by integer add and mask), lo = x - hi exactly; lo goes to the tensor core
+// as it is, which reads its top 10 mantissa bits (2^-21 of x lost)
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  hi = (__float_as_uint(x) + 0x1000u) & 0xffffe000u;
+  lo = __float_as_uint(x - __uint_as_float(hi));
+}
+
+__device__ __forceinline__ void mma_tf32_1688(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// window cell (r, c) holds its 16 columns (problem s: 2s real, 2s + 1
+// imaginary) at (r * 32 + c) * 16 + (n ^ itc_swz(c)): the xor spreads the
+// B-fragment loads of a warp (four consecutive c, eight n) over all banks
+__device__ __forceinline__ int itc_swz(int c) { return ((c >> 1) & 1) << 3; }
+
+static __global__ void __launch_bounds__(256, 2) k_nufft_interp_tc(
+    NufftGeom<float> geo, const ItcTile* __restrict__ tiles, int ntc, const int* __restrict__ perm,
+    const cplx<float>* __restrict__ gall, long gstride, int nx, int ny, double inv_mm,
+    const ProbState* __restrict__ st, int gate, Partials part, int qchi, int nslots, cplx<float>* __restrict__ y2,
+    int B, const double2* __restrict__ ax_base, double2* __restrict__ ax_out) {
+  extern __shared__ __align__(16) float itc_smem[];
+  float* s_g = itc_smem;                                    // [32 * 32 cells][16]
+  float* s_wy = s_g + kItcWin * kItcWin * 2 * kItcProb;     // per warp [16 points][36]
+  float* s_wx = s_wy + 8 * 16 * 36;                         // per warp [32 rows][17] (16 points)
+  __shared__ int s_list[kItcProb];
+  __shared__ int s_cnt[8];
+  __shared__ double s_chi[8][kItcProb];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  // the CTA's points first (independent of the problem chunk): warps over
+  // (block of 16 points, row group); a CTA of nb blocks splits each block's
+  // window rows into ng = 8 / nb contiguous groups, so sparse tiles still
+  // keep all eight warps busy; the groups' sums are added in group order
+  const ItcTile tl = tiles[blockIdx.x];
+  const int nb = (tl.count + 15) >> 4;
+  const int ng = 8 / nb;
+  const int blk = warp % nb, grp = warp / nb;
+  const bool on = grp < ng;
+  const int p0 = tl.start + blk * 16;
+  const int np = on ? min(16, tl.start + tl.count - p0) : 0;
+  int kq = 0, drq = 0, dcq = 0;
+  if (lane < np) {
+    const int pk = perm[p0 + lane];  // point | row offset << 24 | column offset << 27
+    kq = pk & 0xffffff;
+    drq = (pk >> 24) & 7;
+    dcq = (pk >> 27) & 7;
+  }
+  const int nact = active_chunk<kItcProb>(st, gate, B, blockIdx.y, s_list, s_cnt, geo.act_lists);
+  if (nact == 0) return;
+  // chi^2 slots beyond the CTAs (the slot count other kernels of the
+  // operator fill): zero partials
+  if ((int)threadIdx.x < nact && qchi >= 0)
+    for (int sl = blockIdx.x + ntc; sl < nslots; sl += ntc) part.at(qchi, s_list[threadIdx.x])[sl] = 0.0;
+  // the block's separable factors (loads issued before the window's)
+  float fy[16], fx[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const int k = __shfl_sync(0xffffffffu, kq, i);
+    const int dr = __shfl_sync(0xffffffffu, drq, i), dc = __shfl_sync(0xffffffffu, dcq, i);
+    fy[i] = 0.f;
+    fx[i] = 0.f;
+    if (i < np) {
+      const int jy = lane - dc, jx = lane - dr;
+      if (jy >= 0 && jy < kTaps) fy[i] = geo.wy[(size_t)k * kTaps + jy];
+      if (jx >= 0 && jx < kTaps) fx[i] = geo.wx[(size_t)k * kTaps + jx];
+    }
+  }
+  // the epilogue's point data: lane (g, t) finishes points g and g + 8
+  const bool fin = on && grp == 0;
+  int kp[2];
+  double pw[2], pvr[2], pvi[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    kp[h] = __shfl_sync(0xffffffffu, kq, g + 8 * h);
+    pw[h] = pvr[h] = pvi[h] = 0.0;
+    if (fin && g + 8 * h < np) {
+      pw[h] = geo.weight[kp[h]];
+      pvr[h] = geo.vis_r[kp[h]];
+      pvi[h] = geo.vis_i[kp[h]];
+    }
+  }
+  // and the anchors' models the epilogue adds (corrected form)
+  double2 pab[2][2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      pab[h][j] = make_double2(0.0, 0.0);
+      if (ax_base && fin && g + 8 * h < np && 4 * j + t < nact)
+        pab[h][j] = ax_base[(size_t)s_list[4 * j + t] * geo.y2_bstride + kp[h]];
+    }
+  // the window: virtual cell -> stored cell, sign of the imaginary part
+  for (int v = threadIdx.x; v < kItcWin * kItcWin; v += blockDim.x) {
+    const int vr = tl.row0 + (v >> 5), vc = tl.col0 + (v & 31);
+    int cell = -1;
+    float sgn = -1.f;  // NU_SIGN on direct taps
+    int col = half_col(vc, ny);
+    if (col >= 0) {
+      const int row = wrap_row(vr, nx);
+      if (row >= 0) cell = row * (ny + 1) + col;
+    } else {
+      col = half_col(-vc, ny);
+      const int row = wrap_row(-vr, nx);
+      if (col >= 0 && row >= 0) {
+        cell = row * (ny + 1) + col;
+        sgn = 1.f;
+      }
+    }
+    float* dst = s_g + (size_t)v * (2 * kItcProb);
+    const int sw = itc_swz(v & 31);
+    // the four 16-byte stores of a cell in an order rotated by the cell, so
+    // that the 32 lanes of a store instruction cover all banks
+#pragma unroll
+    for (int q4 = 0; q4 < 4; ++q4) {
+      const int s = 2 * ((q4 + (v >> 1)) & 3);
+      float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (cell >= 0) {
+        if (s < nact) {
+          const cplx<float> a = gall[(size_t)s_list[s] * gstride + cell];
+          q.x = a.x;
+          q.y = sgn * a.y;
+        }
+        if (s + 1 < nact) {
+          const cplx<float> a = gall[(size_t)s_list[s + 1] * gstride + cell];
+          q.z = a.x;
+          q.w = sgn * a.y;
+        }
+      }
+      *reinterpret_cast<float4*>(dst + ((2 * s) ^ sw)) = q;
+    }
+  }
+  float* wy_w = s_wy + warp * 16 * 36;
+  float* wx_w = s_wx + warp * kItcWin * 17;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    wy_w[i * 36 + lane] = fy[i];
+    wx_w[lane * 17 + i] = fx[i];
+  }
+  if (lane < kItcProb) s_chi[warp][lane] = 0.0;
+  __syncthreads();
+  const int nj = nact > 4 ? 2 : 1;  // n-tiles of 8 columns (4 problems) in use
+  float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+  if (on) {
+    const int rlo = __reduce_min_sync(0xffffffffu, lane < np ? drq : kItcWin);
+    const int rhi = __reduce_max_sync(0xffffffffu, lane < np ? drq + kTaps - 1 : -1);
+    uint32_t ah[4][4], al[4][4];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        split_tf32(wy_w[(g + 8 * (q & 1)) * 36 + 8 * kk + t + 4 * (q >> 1)], ah[kk][q], al[kk][q]);
+    const int nr = rhi - rlo + 1, per = (nr + ng - 1) / ng;
+    const int r0 = rlo + grp * per, r1 = min(rhi + 1, r0 + per);
+    for (int r = r0; r < r1; ++r) {
+      const float wa = wx_w[r * 17 + g], wb = wx_w[r * 17 + g + 8];
+      const float* grow = s_g + (size_t)r * kItcWin * (2 * kItcProb);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        if (j < nj) {
+          // two accumulation chains (even and odd column groups)
+          float ta[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+          const int n = 8 * j + g;
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {
+            const int c0 = 8 * kk + t, c1 = c0 + 4;
+            uint32_t bh0, bl0, bh1, bl1;
+            split_tf32(grow[c0 * (2 * kItcProb) + (n ^ itc_swz(c0))], bh0, bl0);
+            split_tf32(grow[c1 * (2 * kItcProb) + (n ^ itc_swz(c1))], bh1, bl1);
+            mma_tf32_1688(ta[kk & 1], al[kk], bh0, bh1);
+            mma_tf32_1688(ta[kk & 1], ah[kk], bl0, bl1);
+            mma_tf32_1688(ta[kk & 1], ah[kk], bh0, bh1);
+          }
+          d[j][0] = fmaf(wa, ta[0][0] + ta[1][0], d[j][0]);
+          d[j][1] = fmaf(wa, ta[0][1] + ta[1][1], d[j][1]);
+          d[j][2] = fmaf(wb, ta[0][2] + ta[1][2], d[j][2]);
+          d[j][3] = fmaf(wb, ta[0][3] + ta[1][3], d[j][3]);
+        }
+      }
+    }
+  }
+  // row groups 1.. hand their partial sums to group 0 (through the window's
+  // space: nobody reads it any more)
+  __syncthreads();
+  float* s_part = s_g;  // [8 warps][8 values][32 lanes]
+  if (on && grp > 0) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s_part[(warp * 8 + q) * 32 + lane] = d[q >> 2][q & 3];
+  }
+  __syncthreads();
+  if (fin) {
+    for (int gg = 1; gg < ng; ++gg) {
+      const int w2 = blk + gg * nb;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) d[q >> 2][q & 3] += s_part[(w2 * 8 + q) * 32 + lane];
+    }
+    // epilogue: lane (g, t) holds points g and g + 8, problems 4 j + t
+    double chi[2] = {0.0, 0.0};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (g + 8 * h < np) {
+        const int k = kp[h];
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int slot = 4 * j + t;
+          if (slot < nact) {
+            const size_t e = (size_t)s_list[slot] * geo.y2_bstride + k;
+            double fr = (double)d[j][2 * h] * inv_mm, fi = (double)d[j][2 * h + 1] * inv_mm;
+            if (ax_base) {
+              fr += pab[h][j].x;
+              fi += pab[h][j].y;
+            }
+            if (ax_out) ax_out[e] = make_double2(fr, fi);
+            const double rr = (pvr[h] - fr) * pw[h], ri = (pvi[h] - fi) * pw[h];
+            chi[j] += rr * rr + ri * ri;
+            if (y2) y2[e] = mk<float>((float)(rr * pw[h]), (float)(ri * pw[h]));
+          }
+        }
+      }
+    }
+    // chi^2: over g (fixed butterfly), then over the blocks in order
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      double c = chi[j];
+      c += __shfl_xor_sync(0xffffffffu, c, 4);
+      c += __shfl_xor_sync(0xffffffffu, c, 8);
+      c += __shfl_xor_sync(0xffffffffu, c, 16);
+      if (g == 0) s_chi[warp][4 * j + t] = c;
+    }
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < nact && qchi >= 0) {
+    double c = 0.0;
+    for (int wp = 0; wp < nb; ++wp) c += s_chi[wp][threadIdx.x];
+    part.at(qchi, s_list[threadIdx.x])[blockIdx.x] = c;
+  }
+}
+
 // spreading: one thread-block cluster per (16 x 16 tile, problem chunk); one
 // thread per cell holding the chunk's accumulators.  The tile's point list is
 // split into contiguous segments, one per CTA of the cluster, which bounds
@@ -1178,8 +1455,8 @@ template <typename T> __device__ __forceinline__ int slots_of(const NufftGeom<T>
 
 template <typename T>
 __global__ void k_nufft_resid_model(NufftGeom<T> geo, const double2* __restrict__ az, cplx<T>* __restrict__ y2,
-                                    int shared, int ppw, const ProbState* __restrict__ st, int gate, Partials part,
-                                    int qchi) {
+                                    int shared, int ppw, int nslots, const ProbState* __restrict__ st, int gate,
+                                    Partials part, int qchi) {
   __shared__ double sh[32];
   const int b = blockIdx.y;
   if (!gate_ok(st[b], gate)) return;
@@ -1198,7 +1475,10 @@ __global__ void k_nufft_resid_model(NufftGeom<T> geo, const double2* __restrict_
     // interpolation's order (per warp w in q order, then over w)
     __shared__ double s_t[8][8 * 32];
     const int slot = blockIdx.x * 8 + warp;
-    if (slot >= slots_of(geo, ppw)) return;
+    if (slot >= slots_of(geo, ppw)) {  // a slot beyond the points (padding for another kernel's CTAs)
+      if (lane == 0 && qchi >= 0 && slot < nslots) part.at(qchi, b)[slot] = 0.0;
+      return;
+    }
     const int mtot = geo.pt_hi[0];
     const int n = 8 * ppw, k0 = slot * n;
     for (int l = lane; l < n; l += 32) s_t[warp][l] = (k0 + l < mtot) ? term(k0 + l) : 0.0;

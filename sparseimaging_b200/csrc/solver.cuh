@@ -262,12 +262,25 @@ template <typename T> struct NufftOp : Op {
   // grid, 7 % slower with 16) instead of held in registers; both give the
   // same bits (MFISTA_INTERP_FLY=0 selects the register form)
   bool interp_fly = true;
+  // FP32, shared geometry: interpolation on the tensor cores (k_nufft_interp_tc;
+  // MFISTA_INTERP_TC=0 selects the CUDA-core kernels above)
+  bool interp_tc = false;
+  DevMem d_itc, d_iperm;  // its CTA tiles and the points in tile order
+  int ntc = 0;
+  // chi^2 partial slots every interpolation kernel of this operator writes
+  // (at least its own CTA count; the extra CTAs write zeros), so that the
+  // CUDA-core, tensor-core and FP64 kernels fill the same slots
+  int chi_pad = 0;
   size_t smem_rows = 0, smem_cols = 0;
   long gstride = 0;
   double inv_mm = 0;
 
   NufftOp(Ctx& ctx, const NufftInput& in, bool correct = false) : c(ctx) {
     if (const char* f = getenv("MFISTA_INTERP_FLY")) interp_fly = f[0] == '1';
+    if (sizeof(T) == 4 && in.shared != 0 && in.M < kItcMaxPoints) {
+      const char* f = getenv("MFISTA_INTERP_TC");
+      interp_tc = !(f && f[0] == '0');
+    }
     nx = in.Nx;
     ny = in.Ny;
     B = ctx.B;
@@ -338,6 +351,7 @@ template <typename T> struct NufftOp : Op {
                        [&](int a, int b) { return tptr[a + 1] - tptr[a] > tptr[b + 1] - tptr[b]; });
       d_tord.upload(ord.data(), ord.size());
     }
+    if (interp_tc) build_itc_tiles(mx, my);
     // FFTs: rows as complex length Ny, columns length 2Nx
     fh.init(ny);
     fcol.init(2 * nx);
@@ -362,6 +376,7 @@ template <typename T> struct NufftOp : Op {
     if (correct && sizeof(T) == 4) {
       exact.reset(new NufftOp<double>(ctx, in, false));
       exact->ippw = ippw;  // its chi^2 partials land in the same slots as ours
+      exact->chi_pad = chi_pad;
       d_axa.alloc(sizeof(double2) * (size_t)y2n);
       const char* nm = getenv("MFISTA_NO_MODEL_Z");  // direct forward at z instead (comparison runs)
       model = !(nm && nm[0] == '1');
@@ -391,7 +406,43 @@ template <typename T> struct NufftOp : Op {
     MF_CK(cudaDeviceSynchronize());
   }
 
-  int interp_blocks() const { return std::max(1, cdiv(mmax, shared ? 8 * ippw : 8)); }
+  int interp_blocks() const { return std::max({1, cdiv(mmax, shared ? 8 * ippw : 8), chi_pad}); }
+
+  // Tensor-core interpolation tiles: every point binned by its first tap
+  // (mx - 11, my - 11) into an 8 x 8 tile of the virtual grid; a tile's
+  // points in (mx, my, index) order, cut into CTAs of at most kItcPts.
+  void build_itc_tiles(const std::vector<int>& mx, const std::vector<int>& my) {
+    auto fdiv = [](int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); };
+    std::vector<int> ord(mtot);
+    for (int k = 0; k < mtot; ++k) ord[k] = k;
+    auto key = [&](int k) {
+      return std::make_tuple(fdiv(mx[k] - (kMSP - 1), kItcTile), fdiv(my[k] - (kMSP - 1), kItcTile), mx[k], my[k]);
+    };
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return key(a) < key(b); });
+    std::vector<ItcTile> tiles;
+    for (int i = 0; i < mtot;) {
+      const int tr = fdiv(mx[ord[i]] - (kMSP - 1), kItcTile), tcol = fdiv(my[ord[i]] - (kMSP - 1), kItcTile);
+      int j = i;
+      while (j < mtot && fdiv(mx[ord[j]] - (kMSP - 1), kItcTile) == tr &&
+             fdiv(my[ord[j]] - (kMSP - 1), kItcTile) == tcol)
+        ++j;
+      for (int a = i; a < j; a += kItcPts) tiles.push_back(ItcTile{tr * kItcTile, tcol * kItcTile, a, std::min(kItcPts, j - a)});
+      i = j;
+    }
+    // launch order: fullest CTAs first, so that the last wave holds short ones
+    std::stable_sort(tiles.begin(), tiles.end(), [](const ItcTile& a, const ItcTile& b) { return a.count > b.count; });
+    ntc = (int)tiles.size();
+    chi_pad = std::max(chi_pad, ntc);
+    std::vector<int> packed(std::max(mtot, 1), 0);
+    for (const ItcTile& tl : tiles)
+      for (int a = tl.start; a < tl.start + tl.count; ++a) {
+        const int k = ord[a];
+        packed[a] = k | ((mx[k] - (kMSP - 1) - tl.row0) << 24) | ((my[k] - (kMSP - 1) - tl.col0) << 27);
+      }
+    d_itc.upload(tiles.data(), std::max<size_t>(tiles.size(), 1));
+    d_iperm.upload(packed.data(), packed.size());
+    set_smem(k_nufft_interp_tc, kItcSmem);
+  }
   int interp_chunks() const { return cdiv(B, SharedChunk<T>::kInterp); }
   static constexpr int kMaxInterpPpw = 32;
   static size_t spread_smem() { return sizeof(cplx<T>) * SharedChunk<T>::kSpread * 256; }
@@ -411,7 +462,11 @@ template <typename T> struct NufftOp : Op {
     // problem at a time.  Both chunk the batch's active problems.
     if (shared) {
       if constexpr (sizeof(T) == 4) {
-        if (interp_fly)
+        if (interp_tc)
+          k_nufft_interp_tc<<<dim3(ntc, cdiv(B, kItcProb)), 256, kItcSmem, s>>>(
+              geo, d_itc.as<ItcTile>(), ntc, d_iperm.as<int>(), g, gstride, nx, ny, inv_mm, c.st, gate, c.part, qchi,
+              chi_slots(), y2, B, base, out);
+        else if (interp_fly)
           k_nufft_interp_group_fly<T><<<dim3(interp_blocks(), interp_chunks()), 256, 0, s>>>(
               geo, g, gstride, nx, ny, inv_mm, c.st, gate, c.part, qchi, y2, B, base, out, ippw);
         else
@@ -459,7 +514,7 @@ template <typename T> struct NufftOp : Op {
   void forward_z(cudaStream_t s, int gate, int qchi) override {
     const int gx = shared ? cdiv(chi_slots(), 8) : chi_slots();
     k_nufft_resid_model<T><<<dim3(gx, B), 256, 0, s>>>(geo, d_az.as<double2>(), d_y2.as<cplx<T>>(), shared ? 1 : 0,
-                                                        ippw, c.st, gate, c.part, qchi);
+                                                        ippw, chi_slots(), c.st, gate, c.part, qchi);
     MF_LAUNCH_CK();
   }
 
@@ -537,7 +592,7 @@ template <typename T> struct NufftOp : Op {
   }
 
   int chi_slots() const override { return interp_blocks(); }
-  int max_chi_slots() const override { return std::max(1, cdiv(mmax, 8)); }
+  int max_chi_slots() const override { return std::max({1, cdiv(mmax, 8), chi_pad}); }
   int tsv_slots() const override { return nx; }  // row-pass CTAs at rows_per_cta = 1
 
   LaunchShapes shapes() const override {
@@ -1119,10 +1174,18 @@ struct Solver {
     d_wt.upload(w.data(), w.size());
     d_jq.alloc(sizeof(double) * (size_t)ctx.B * kNumQ);
   }
+  // every thresholded pixel f is scaled by mask[f] (mask: [N], shared by
+  // all problems)
+  void set_mask(const double* mask) {
+    d_mask.upload(mask, (size_t)ctx.N);
+    mask_ptr = d_mask.as<double>();
+  }
   // device loop with conditional IF blocks: the refresh and gradient blocks
   // run only in steps where some problem needs them (k_select_blocks)
   bool cond_blocks = false;
   const float* box_ptr = nullptr;
+  DevMem d_mask;
+  const double* mask_ptr = nullptr;  // pixel scale of the thresholded image (movie c_box), or null
 
   Solver() {}
   ~Solver() {
@@ -1407,7 +1470,7 @@ struct Solver {
     }
     // trial point
     if (form == kFormTSV) {
-      k_update_tsv<<<ig, 256, 0, s>>>(ctx.z, ctx.dfdx, ctx.xnew, dm, ctx.prm, ctx.st, box_ptr, ctx.part);
+      k_update_tsv<<<ig, 256, 0, s>>>(ctx.z, ctx.dfdx, ctx.xnew, dm, ctx.prm, ctx.st, box_ptr, mask_ptr, ctx.part);
       MF_LAUNCH_CK();
       if (joint) {
         k_movie_dx<<<ig, 256, 0, s>>>(ctx.xnew, dm, d_wt.as<double>(), ctx.st, kGateTrial, ctx.part);
@@ -1609,7 +1672,8 @@ struct Solver {
       if (kernel == 6) {
         dim3 ig(img_blocks(), ctx.B);
         if (form == kFormTSV) {
-          k_update_tsv<<<ig, 256, 0, stream>>>(ctx.z, ctx.dfdx, ctx.xnew, dm, ctx.prm, ctx.st, box_ptr, ctx.part);
+          k_update_tsv<<<ig, 256, 0, stream>>>(ctx.z, ctx.dfdx, ctx.xnew, dm, ctx.prm, ctx.st, box_ptr, mask_ptr,
+                                                ctx.part);
           MF_LAUNCH_CK();
         } else {
           launch_fgp(stream);

@@ -50,8 +50,12 @@ def test_fp32_form_image_error_matches_fp64(gpulib):
         assert all(r["finalcost"] <= t for r, t in zip(R, targets))
     e64, e32 = _errors(X64, xs), _errors(X32, xs)
     nz = np.array([np.linalg.norm(x) > 0 for x in xs])
-    # the zero solutions (lambda above max|A^H y|) stay exactly zero
-    assert np.all(e64[~nz] == 0) and np.all(e32[~nz] == 0)
+    # the zero solutions: the grid's largest lambda_l1 is max|A^H y| itself,
+    # where FP64 keeps x = 0 exactly and an FP32 gradient may pass the
+    # threshold by a rounding (measured: one pixel at 7.8e-12, 1e-8 of the
+    # images' peak); hold it to 1e-6 of the median peak of x*
+    scale = float(np.median([np.abs(x).max() for x in xs[nz]]))
+    assert np.all(e64[~nz] == 0) and np.all(e32[~nz] <= 1e-6 * scale)
     bound = np.maximum(1e-4, 1.05 * e64)
     bad = [(b, e32[b], e64[b]) for b in range(len(xs)) if e32[b] > bound[b]]
     assert not bad, bad

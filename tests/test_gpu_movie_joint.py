@@ -75,6 +75,42 @@ def test_frame_times_scale_the_temporal_weight(gpulib):
     assert [r["ITER"] for r in a[1]] == [r["ITER"] for r in b[1]]
 
 
+def test_movie_c_box_matches_oracle(gpulib):
+    """c_box as the matlab code applies it: xinit .* c_box, and every
+    thresholded image times c_box (a support mask with fractional edges)."""
+    nx, T = 32, 3
+    fr, geo, off = _movie(T, nx, seed=11)
+    lam, lip = _params(gpulib, fr, nx)
+    lt = 5.0 * lam
+    yy, xx = np.divmod(np.arange(nx * nx), nx)
+    r2 = (yy - nx / 2) ** 2 + (xx - nx / 2) ** 2
+    box = np.where(r2 <= (nx / 3) ** 2, 1.0, np.where(r2 <= (nx / 2.5) ** 2, 0.5, 0.0))
+    x0 = np.full(nx * nx, 1e-4)
+    X, R, tcost = gpulib.nufft_movie(*geo, off, nx, nx, lam, 1e-2 * lam, lt, lip, 200, 0.0, xinit=x0, c_box=box)
+    frames = [(f.u_dx, f.v_dy, f.vis_r, f.vis_i, f.vis_std) for f in fr]
+    Xo, it, c, cost = MO.movie(frames, nx, nx, lam, 1e-2 * lam, lt, lip, 200, 0.0, xinit=x0, c_box=box)
+    assert all(r["ITER"] == it for r in R)
+    assert rel(X, Xo) < 1e-8
+    assert np.all(X[:, box == 0] == 0)
+
+
+def test_movie_fp32_form(gpulib):
+    """The FP32 form of the joint movie (corrected FP32 NUFFTs, FP64 control)
+    reaches the FP64 form's objective: the same stopping rule on the summed
+    objective, final objectives within 1e-6 relative."""
+    nx, T = 32, 4
+    fr, geo, off = _movie(T, nx, seed=13)
+    lam, lip = _params(gpulib, fr, nx)
+    lt = 5.0 * lam
+    out = {}
+    for prec in (gpulib.FP64, gpulib.FP32):
+        X, R, tcost = gpulib.nufft_movie(*geo, off, nx, nx, lam, 1e-2 * lam, lt, lip, 3000, 1e-9, precision=prec)
+        out[prec] = (X, sum(r["finalcost"] for r in R) + tcost, R[0]["ITER"])
+    f64, f32 = out[gpulib.FP64][1], out[gpulib.FP32][1]
+    assert abs(f32 - f64) <= 1e-6 * f64
+    assert rel(out[gpulib.FP32][0], out[gpulib.FP64][0]) < 1e-2
+
+
 def test_movie_rejects_bad_frame_times(gpulib):
     nx, T = 32, 3
     fr, geo, off = _movie(T, nx, seed=8)

@@ -50,3 +50,26 @@ def test_coupled_movie_properties():
         assert np.all(np.diff(cost) <= 0)          # MFISTA keeps the objective monotone
         out[lt] = MO.d_x(X, np.ones(2))
     assert out[10.0 * lam] < out[0.0]
+
+
+def test_c_box_support_and_scaling():
+    """c_box (matlab/MFISTA_movie_eht.m:46, :143-146): ones change nothing,
+    a 0/1 mask keeps the pixels outside it at zero, and the frames stay
+    monotone with fractional weights."""
+    nx = 16
+    fr, frames = _frames(2, nx, seed=5)
+    lam, lip = _lams(fr[0], nx)
+    lip *= 1.5
+    args = (frames, nx, nx, lam, 1e-2 * lam, 5.0 * lam, lip, 80, 0.0)
+    X0, it0, _, _ = MO.movie(*args)
+    X1, it1, _, _ = MO.movie(*args, c_box=np.ones(nx * nx))
+    assert it0 == it1 and np.array_equal(X0, X1)
+    yy, xx = np.divmod(np.arange(nx * nx), nx)
+    mask = ((yy - nx / 2) ** 2 + (xx - nx / 2) ** 2 <= (nx / 3) ** 2).astype(np.float64)
+    Xm, _, _, cost = MO.movie(*args, c_box=mask, xinit=np.full(nx * nx, 1e-3))
+    assert np.all(Xm[:, mask == 0] == 0)
+    assert np.any(Xm[:, mask == 1] != 0)
+    assert np.all(np.diff(cost) <= 0)
+    w = 0.5 + 0.5 * mask
+    Xw, _, _, cost = MO.movie(*args, c_box=w)
+    assert np.all(np.diff(cost) <= 0)
