@@ -1229,6 +1229,178 @@ static __global__ void __launch_bounds__(256, 2) k_nufft_interp_tc(
   }
 }
 
+// ---------------------------------------------------------------------------
+// Spreading on the tensor cores (FP32 form, shared geometry)
+//
+// Output-stationary like k_nufft_spread_shared, in matrix form: the grid is
+// cut into tiles of 8 rows x 16 columns of the stored half plane; a cell's
+// value is a sum over "virtual points": every uv point once as itself
+// (direct taps, first tap (mx - 11, my - 11), imaginary part negated: the
+// reference's NU_SIGN) and once mirrored (first tap (-mx - 12, -my - 12),
+// both weight vectors reversed, imaginary part kept), each with half the
+// residual.  A tile's list holds every virtual point with a tap on it
+// (built on the host), so a cell (row r, column c) with virtual coordinates
+// (mr, mc) (the reference's wrap: mr = r or r - 2Nx, mc = c or -Ny) is
+//   sum_p wy_p[mc - my0_p] * (wx_p[mr - mx0_p] * y_p)      (taps outside: 0)
+// For one row that is a 16 (columns) x K (points) by K x 16 (problem
+// columns) product: warp w of the CTA takes tile row w and runs it as
+// mma.sync m16n8k8 TF32 with the operands split in two TF32 parts
+// (lo*hi + hi*lo + hi*hi, FP32 accumulation).  Points are staged 64 at a
+// time; the column weights (the A operand, shared by the eight rows) are
+// formed once per stage for all warps.  Long lists are cut into segments of
+// kStcSeg points run by separate CTAs, which leave their partial tiles in a
+// scratch buffer; the last of a tile's CTAs to finish (a ticket per tile and
+// problem chunk) adds the segments in segment order and writes the tile, so
+// the result does not depend on the order the CTAs ran in.
+// ---------------------------------------------------------------------------
+constexpr int kStcRows = 8, kStcCols = 16;
+constexpr int kStcProb = 8;   // problems per CTA (16 real columns)
+constexpr int kStcStage = 64; // virtual points per stage
+constexpr int kStcSeg = 256;  // virtual points per CTA (longer lists are cut)
+struct StcItem {
+  int tile;           // tile index (row-major over tile rows x tile columns)
+  int start, count;   // the segment's virtual points: list[start, start + count)
+  int seg, nseg;      // segment index and count of this tile
+  int scratch;        // scratch slot of segment 0 of the tile (nseg > 1)
+};
+
+static __global__ void __launch_bounds__(256) k_nufft_spread_tc(
+    NufftGeom<float> geo, const StcItem* __restrict__ items, const int* __restrict__ vlist,
+    const cplx<float>* __restrict__ y2, cplx<float>* __restrict__ gall, long gstride, int nx, int ny,
+    int ntcol, const ProbState* __restrict__ st, int gate, int B, float* __restrict__ scratch,
+    unsigned int* __restrict__ tickets) {
+  __shared__ float s_ah[kStcStage * 24], s_al[kStcStage * 24];  // [point][16 columns] (row stride 24)
+  __shared__ float s_y[kStcStage * 24];                          // [point][16 problem columns]
+  __shared__ float s_bx[8][kStcStage];                           // per warp (tile row): wx at that row
+  __shared__ int s_k[kStcStage], s_x0[kStcStage], s_y0[kStcStage], s_fl[kStcStage];
+  __shared__ int s_list[kStcProb];
+  __shared__ int s_cnt[8];
+  __shared__ unsigned int s_ticket;
+  const int nact = active_chunk<kStcProb>(st, gate, B, blockIdx.y, s_list, s_cnt, geo.act_lists);
+  if (nact == 0) return;
+  const StcItem it = items[blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int tr = it.tile / ntcol, tcl = it.tile - tr * ntcol;
+  const int row = tr * kStcRows + warp;
+  const bool row_ok = row < 2 * nx;
+  const int mrow = row < nx ? row : row - 2 * nx;
+  const int nj = nact > 4 ? 2 : 1;
+  float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+  for (int base = it.start; base < it.start + it.count; base += kStcStage) {
+    const int np = min(kStcStage, it.start + it.count - base);
+    // the stage's virtual points
+    if (threadIdx.x < kStcStage) {
+      const int q = threadIdx.x;
+      int k = 0, x0 = 1 << 29, y0 = 1 << 29, fl = 0;  // padding: no tap anywhere
+      if (q < np) {
+        const int e = vlist[base + q];
+        k = e & 0xffffff;
+        fl = (e >> 24) & 1;
+        const int mx = geo.mx[k], my = geo.my[k];
+        x0 = fl ? -mx - kMSP : mx - (kMSP - 1);
+        y0 = fl ? -my - kMSP : my - (kMSP - 1);
+      }
+      s_k[q] = k;
+      s_x0[q] = x0;
+      s_y0[q] = y0;
+      s_fl[q] = fl;
+    }
+    __syncthreads();
+    // column weights (A operand) for the whole CTA, split hi / lo
+    for (int e = threadIdx.x; e < kStcStage * kStcCols; e += blockDim.x) {
+      const int q = e >> 4, cc = e & 15;
+      const int col = tcl * kStcCols + cc;
+      const int mcol = col < ny ? col : -ny;
+      const int jy = mcol - s_y0[q];
+      float w = 0.f;
+      if (col <= ny && jy >= 0 && jy < kTaps) w = geo.wy[(size_t)s_k[q] * kTaps + (s_fl[q] ? kTaps - 1 - jy : jy)];
+      uint32_t hi, lo;
+      split_tf32(w, hi, lo);
+      s_ah[q * 24 + cc] = __uint_as_float(hi);
+      s_al[q * 24 + cc] = __uint_as_float(lo);
+    }
+    // the chunk's half residuals, imaginary sign of direct / mirrored taps
+    for (int e = threadIdx.x; e < kStcStage * 2 * kStcProb; e += blockDim.x) {
+      const int q = e >> 4, n = e & 15, sl = n >> 1;
+      float v = 0.f;
+      if (q < np && sl < nact) {
+        const cplx<float> r = y2[(size_t)s_list[sl] * geo.y2_bstride + s_k[q]];
+        v = (n & 1) ? (s_fl[q] ? 0.5f * r.y : -0.5f * r.y) : 0.5f * r.x;
+      }
+      s_y[q * 24 + n] = v;
+    }
+    // this warp's row weights
+    for (int q = lane; q < kStcStage; q += 32) {
+      const int jx = mrow - s_x0[q];
+      float w = 0.f;
+      if (row_ok && jx >= 0 && jx < kTaps) w = geo.wx[(size_t)s_k[q] * kTaps + (s_fl[q] ? kTaps - 1 - jx : jx)];
+      s_bx[warp][q] = w;
+    }
+    __syncthreads();
+    const int nk = (np + 7) & ~7;
+    for (int kb = 0; kb < nk; kb += 8) {
+      const int p0 = (kb + t) * 24, p1 = (kb + t + 4) * 24;
+      uint32_t ah[4], al[4];
+      ah[0] = __float_as_uint(s_ah[p0 + g]);
+      ah[1] = __float_as_uint(s_ah[p0 + g + 8]);
+      ah[2] = __float_as_uint(s_ah[p1 + g]);
+      ah[3] = __float_as_uint(s_ah[p1 + g + 8]);
+      al[0] = __float_as_uint(s_al[p0 + g]);
+      al[1] = __float_as_uint(s_al[p0 + g + 8]);
+      al[2] = __float_as_uint(s_al[p1 + g]);
+      al[3] = __float_as_uint(s_al[p1 + g + 8]);
+      const float bx0 = s_bx[warp][kb + t], bx1 = s_bx[warp][kb + t + 4];
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        if (j < nj) {
+          uint32_t bh0, bl0, bh1, bl1;
+          split_tf32(bx0 * s_y[p0 + 8 * j + g], bh0, bl0);
+          split_tf32(bx1 * s_y[p1 + 8 * j + g], bh1, bl1);
+          mma_tf32_1688(d[j], al, bh0, bh1);
+          mma_tf32_1688(d[j], ah, bl0, bl1);
+          mma_tf32_1688(d[j], ah, bh0, bh1);
+        }
+      }
+    }
+    __syncthreads();  // the next stage overwrites the staged points
+  }
+  // lane (g, t) holds columns g and g + 8 of its row, problems 4 j + t
+  const size_t cstride = (size_t)gridDim.y * 2048;
+  if (it.nseg > 1) {
+    float* mine = scratch + (size_t)(it.scratch + it.seg) * cstride + (size_t)blockIdx.y * 2048;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) mine[(warp * 32 + lane) * 8 + q] = d[q >> 2][q & 3];
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_ticket = atomicAdd(&tickets[(size_t)it.tile * gridDim.y + blockIdx.y], 1u);
+    __syncthreads();
+    if (s_ticket != (unsigned int)(it.nseg - 1)) return;
+    __threadfence();
+#pragma unroll
+    for (int q = 0; q < 8; ++q) d[q >> 2][q & 3] = 0.f;
+    for (int s = 0; s < it.nseg; ++s) {
+      const float* part = scratch + (size_t)(it.scratch + s) * cstride + (size_t)blockIdx.y * 2048;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) d[q >> 2][q & 3] += __ldcg(part + (warp * 32 + lane) * 8 + q);
+    }
+    if (threadIdx.x == 0) tickets[(size_t)it.tile * gridDim.y + blockIdx.y] = 0u;  // for the next launch
+  }
+  if (!row_ok) return;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int col = tcl * kStcCols + g + 8 * h;
+    if (col <= ny) {
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int sl = 4 * j + t;
+        if (sl < nact)
+          gall[(size_t)s_list[sl] * gstride + (size_t)row * (ny + 1) + col] = mk<float>(d[j][2 * h], d[j][2 * h + 1]);
+      }
+    }
+  }
+}
+
 // spreading: one thread-block cluster per (16 x 16 tile, problem chunk); one
 // thread per cell holding the chunk's accumulators.  The tile's point list is
 // split into contiguous segments, one per CTA of the cluster, which bounds

@@ -267,6 +267,11 @@ template <typename T> struct NufftOp : Op {
   bool interp_tc = false;
   DevMem d_itc, d_iperm;  // its CTA tiles and the points in tile order
   int ntc = 0;
+  // FP32, shared geometry: spreading on the tensor cores (k_nufft_spread_tc;
+  // MFISTA_SPREAD_TC=0 selects the cluster kernel)
+  bool spread_tc = false;
+  DevMem d_sitems, d_svlist, d_sscratch, d_stickets;
+  int nsitems = 0, stc_cols = 0;
   // chi^2 partial slots every interpolation kernel of this operator writes
   // (at least its own CTA count; the extra CTAs write zeros), so that the
   // CUDA-core, tensor-core and FP64 kernels fill the same slots
@@ -280,6 +285,8 @@ template <typename T> struct NufftOp : Op {
     if (sizeof(T) == 4 && in.shared != 0 && in.M < kItcMaxPoints) {
       const char* f = getenv("MFISTA_INTERP_TC");
       interp_tc = !(f && f[0] == '0');
+      const char* f2 = getenv("MFISTA_SPREAD_TC");
+      spread_tc = !(f2 && f2[0] == '0');
     }
     nx = in.Nx;
     ny = in.Ny;
@@ -352,6 +359,7 @@ template <typename T> struct NufftOp : Op {
       d_tord.upload(ord.data(), ord.size());
     }
     if (interp_tc) build_itc_tiles(mx, my);
+    if (spread_tc) build_stc_items(mx, my);
     // FFTs: rows as complex length Ny, columns length 2Nx
     fh.init(ny);
     fcol.init(2 * nx);
@@ -407,6 +415,56 @@ template <typename T> struct NufftOp : Op {
   }
 
   int interp_blocks() const { return std::max({1, cdiv(mmax, shared ? 8 * ippw : 8), chi_pad}); }
+
+  // Tensor-core spreading: each 8 x 16 tile of the stored half grid lists
+  // the virtual points (point | mirrored << 24) with a tap on it, in (point,
+  // mirrored) order; a tile's list is cut into CTA segments of kStcSeg.
+  void build_stc_items(const std::vector<int>& mx, const std::vector<int>& my) {
+    const int ntr = cdiv(2 * nx, kStcRows);
+    stc_cols = cdiv(ny + 1, kStcCols);
+    const int nt = ntr * stc_cols;
+    std::vector<std::vector<int>> lists(nt);
+    std::vector<int> trs, tcs;
+    for (int k = 0; k < mtot; ++k)
+      for (int fl = 0; fl < 2; ++fl) {
+        const int x0 = fl ? -mx[k] - kMSP : mx[k] - (kMSP - 1);
+        const int y0 = fl ? -my[k] - kMSP : my[k] - (kMSP - 1);
+        trs.clear();
+        tcs.clear();
+        for (int v = x0; v < x0 + kTaps; ++v) {  // stored rows of the taps (the reference's wrap)
+          const int r = (v >= 0 && v < nx) ? v : (v >= -nx && v < 0) ? v + 2 * nx : -1;
+          if (r >= 0 && (trs.empty() || trs.back() != r / kStcRows)) trs.push_back(r / kStcRows);
+        }
+        for (int v = y0; v < y0 + kTaps; ++v) {  // stored columns (0..Ny-1 direct, -Ny -> Ny)
+          const int c = (v >= 0 && v < ny) ? v : (v == -ny) ? ny : -1;
+          if (c >= 0 && std::find(tcs.begin(), tcs.end(), c / kStcCols) == tcs.end()) tcs.push_back(c / kStcCols);
+        }
+        std::sort(trs.begin(), trs.end());
+        trs.erase(std::unique(trs.begin(), trs.end()), trs.end());
+        for (int a : trs)
+          for (int b : tcs) lists[(size_t)a * stc_cols + b].push_back(k | (fl << 24));
+      }
+    std::vector<int> flat;
+    std::vector<StcItem> items;
+    int nscr = 0;
+    for (int t = 0; t < nt; ++t) {
+      const int start = (int)flat.size(), cnt = (int)lists[t].size();
+      flat.insert(flat.end(), lists[t].begin(), lists[t].end());
+      const int nseg = std::max(1, cdiv(cnt, kStcSeg));
+      for (int sg = 0; sg < nseg; ++sg)
+        items.push_back(StcItem{t, start + sg * kStcSeg, std::min(kStcSeg, cnt - sg * kStcSeg), sg, nseg, nscr});
+      if (nseg > 1) nscr += nseg;
+    }
+    // launch order: longest segments first
+    std::stable_sort(items.begin(), items.end(), [](const StcItem& a, const StcItem& b) { return a.count > b.count; });
+    nsitems = (int)items.size();
+    d_sitems.upload(items.data(), items.size());
+    d_svlist.upload(flat.data(), std::max<size_t>(flat.size(), 1));
+    const int chunks = cdiv(B, kStcProb);
+    d_sscratch.alloc(sizeof(float) * (size_t)std::max(nscr, 1) * chunks * 2048);
+    d_stickets.alloc(sizeof(unsigned int) * (size_t)nt * chunks);
+    MF_CK(cudaMemset(d_stickets.p, 0, d_stickets.bytes));
+  }
 
   // Tensor-core interpolation tiles: every point binned by its first tap
   // (mx - 11, my - 11) into an 8 x 8 tile of the virtual grid; a tile's
@@ -544,6 +602,15 @@ template <typename T> struct NufftOp : Op {
 
   void launch_spread(cudaStream_t s, cplx<T>* g, int gate) {
     const NufftGeom<T> geo = geo_now();
+    if constexpr (sizeof(T) == 4) {
+      if (spread_tc) {
+        k_nufft_spread_tc<<<dim3(nsitems, cdiv(B, kStcProb)), 256, 0, s>>>(
+            geo, d_sitems.as<StcItem>(), d_svlist.as<int>(), d_y2.as<cplx<float>>(), g, gstride, nx, ny, stc_cols,
+            c.st, gate, B, d_sscratch.as<float>(), d_stickets.as<unsigned int>());
+        MF_LAUNCH_CK();
+        return;
+      }
+    }
     if (shared) {
       // cluster of spread_cs CTAs per tile, each a segment of its points
       cudaLaunchConfig_t cfg = {};

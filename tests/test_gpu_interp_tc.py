@@ -1,5 +1,5 @@
-"""Tensor-core interpolation (FP32 form, k_nufft_interp_tc) against the
-CUDA-core FP32 kernel and the FP64 operator.
+"""Tensor-core interpolation and spreading (FP32 form, k_nufft_interp_tc,
+k_nufft_spread_tc) against the CUDA-core FP32 kernels and the FP64 operator.
 
 The tensor-core kernel stages each tile's 32 x 32 window of virtual cells
 (wrapped rows, Hermitian-mirrored columns with the conjugate, dropped taps
@@ -7,7 +7,10 @@ as zeros) and takes the separable tap sums as 3-pass TF32 products, so it
 must agree with the per-tap FP32 kernel to FP32 rounding (2e-6 relative L2)
 and with FP64 as every FP32 operator does (2e-5).  The geometries cover
 the lambda-grid workload, non-power-of-two grids, points near the Nyquist
-edges (taps dropped or mirrored) and points on the v = 0 fold.
+edges (taps dropped or mirrored) and points on the v = 0 fold.  The
+tensor-core spreading sums every stored cell over the "virtual points"
+(each point direct and mirrored) listed for its 8 x 16 tile, long lists in
+segments added by the last CTA of the tile: the same bounds.
 """
 import os
 
@@ -19,17 +22,26 @@ from conftest import rel
 pytestmark = pytest.mark.gpu
 
 
-def _forward(gpulib, u, v, nx, x, tc):
-    old = os.environ.get("MFISTA_INTERP_TC")
-    os.environ["MFISTA_INTERP_TC"] = "1" if tc else "0"
+def _with_env(name, on, fn):
+    old = os.environ.get(name)
+    os.environ[name] = "1" if on else "0"
     try:
-        fr, fi = gpulib.nufft_forward(u, v, nx, nx, x, precision=gpulib.FP32)
+        return fn()
     finally:
         if old is None:
-            del os.environ["MFISTA_INTERP_TC"]
+            del os.environ[name]
         else:
-            os.environ["MFISTA_INTERP_TC"] = old
+            os.environ[name] = old
+
+
+def _forward(gpulib, u, v, nx, x, tc):
+    fr, fi = _with_env("MFISTA_INTERP_TC", tc, lambda: gpulib.nufft_forward(u, v, nx, nx, x, precision=gpulib.FP32))
     return fr + 1j * fi
+
+
+def _adjoint(gpulib, u, v, nx, a, b, tc):
+    return _with_env("MFISTA_SPREAD_TC", tc,
+                     lambda: gpulib.nufft_adjoint(u, v, nx, nx, a, b, precision=gpulib.FP32))
 
 
 def _geometries():
@@ -61,5 +73,17 @@ def test_tensor_core_interpolation_matches(gpulib, case):
     cc = _forward(gpulib, u, v, nx, x, False)
     fr, fi = gpulib.nufft_forward(u, v, nx, nx, x)
     f64 = fr + 1j * fi
+    assert rel(tc, cc) < 2e-6, name
+    assert rel(tc, f64) < 2e-5, name
+
+
+@pytest.mark.parametrize("case", range(6))
+def test_tensor_core_spreading_matches(gpulib, case):
+    name, u, v, nx = _geometries()[case]
+    rng = np.random.default_rng(100 + case)
+    a, b = rng.standard_normal(u.size), rng.standard_normal(u.size)
+    tc = _adjoint(gpulib, u, v, nx, a, b, True)
+    cc = _adjoint(gpulib, u, v, nx, a, b, False)
+    f64 = gpulib.nufft_adjoint(u, v, nx, nx, a, b)
     assert rel(tc, cc) < 2e-6, name
     assert rel(tc, f64) < 2e-5, name
