@@ -121,7 +121,13 @@ def dft_lambda_grid(si):
         secs = R[0]["comp_time"]
         out[name] = {"solves_per_s": round(len(grid) / secs, 3), "solve_s": round(secs, 4),
                      "reached_1e-6": int(sum(r["finalcost"] <= t for r, t in zip(R, targets))),
-                     "max_iters": int(max(r["ITER"] for r in R))}
+                     "max_iters": int(max(r["ITER"] for r in R)),
+                     # the problems that stopped above their target: which lambda,
+                     # how far from F*, after how many iterations (the stop rule
+                     # with eps = 0 ends a solve whose objective no longer falls)
+                     "not_reached": [{"problem": b, "lambda_l1": float(grid[b][0]), "lambda_tsv": float(grid[b][1]),
+                                      "rel_gap_to_fstar": float(r["finalcost"] / fx["fstar"][b] - 1), "iters": int(r["ITER"])}
+                                     for b, (r, t) in enumerate(zip(R, targets)) if r["finalcost"] > t]}
     out["speedup_bf16x6_vs_fp64"] = round(out["fp64"]["solve_s"] / out["bf16x6"]["solve_s"], 2)
     out["looe"] = dft_looe_side(si, p, X64, [float(lt) for _, lt in grid])
     return out
@@ -186,6 +192,30 @@ def movie_batch(si):
             "fp32_vs_fp64_rel_objective": {"median": float(np.median(dobj)), "max": float(max(dobj))},
             "fp32_vs_fp64_rel_image": {"median": float(np.median(dimg)), "max": float(max(dimg))},
             "joint": _reported(movie_joint, si, geo, off, probs)}
+
+
+def dropin_calls(si):
+    """Cost of the drop-in entry outside the solve: mfista_imaging_core_nufft
+    on config 0 (64 x 64, tests/golden/c0_nufft.npz, 300 iterations) called
+    three times: building its solver (first call), reusing the kept solver
+    with new visibilities (second call), and with the cache off; wall time
+    of the call against the solve time it reports (comp_time)."""
+    g = np.load(os.path.join(ROOT, "tests", "golden", "c0_nufft.npz"))
+    args = lambda vr: (g["u"], g["v"], vr, g["vis_i"], g["vis_std"], 64, 64, 300, 1e-5, float(g["lam1"]), 0.0,
+                       float(g["lamt"]), float(g["cinit"]))
+    out = {"workload": "config 0: 64x64, M = %d, 300 iterations per call" % g["u"].size}
+    si.release_cache()
+    for name, vr, env in (("first_call", g["vis_r"], "1"), ("same_geometry", 0.9 * g["vis_r"], "1"),
+                          ("cache_off", 0.9 * g["vis_r"], "0")):
+        os.environ["MFISTA_DROPIN_CACHE"] = env
+        t = time.perf_counter()
+        _, r = si.imaging_core_nufft(*args(vr))
+        wall = time.perf_counter() - t
+        out[name] = {"wall_s": round(wall, 4), "solve_s": round(r["comp_time"], 4),
+                     "outside_solve_s": round(wall - r["comp_time"], 4), "iters": r["ITER"]}
+    os.environ.pop("MFISTA_DROPIN_CACHE", None)
+    si.release_cache()
+    return out
 
 
 def _reported(fn, *args):
@@ -634,7 +664,7 @@ def run_ours(args):
     if rank == 0:  # side measurements of the other configurations (rank 0 only)
         for key, fn in (("dft_lambda_grid", dft_lambda_grid), ("movie_batch", movie_batch),
                         ("fft_tv_fgp50", lambda s_: fft_config1(s_, hbm)),
-                        ("warmstart_config4", warmstart_config4)):
+                        ("warmstart_config4", warmstart_config4), ("dropin_calls", dropin_calls)):
             try:
                 side[key] = fn(si)
             except Exception as e:  # reported, not required

@@ -107,6 +107,14 @@ int mfista_set_device(int device);
 int mfista_last_status(void);
 const char *mfista_last_error(void);
 
+/* mfista_imaging_core_nufft keeps the solvers of its last calls (at most 4,
+ * per device): a call with the same uv points, vis_std, sizes, regulariser
+ * form, FGP iterations and box mask as a kept one reuses its device buffers
+ * and captured solve graph and only uploads the new visibilities.  This
+ * frees them (solvers in use by another thread stay).  Setting
+ * MFISTA_DROPIN_CACHE=0 in the environment disables the cache. */
+void mfista_release_cache(void);
+
 /* FGP iterations used by the TV form of the drop-in entry points on this
  * thread (the reference compiles it in: FGPITER 100, c/mfista.h:38).
  * Returns the previous value; n < 1 is rejected (returns -1). */

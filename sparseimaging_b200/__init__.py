@@ -137,6 +137,8 @@ def lib():
         L.mfista_dft_apply.argtypes = [_dp, C.c_int, C.c_int, _dp, C.c_int, C.c_int, C.c_int, _dp]
         L.mfista_dft_profile.restype = C.c_int
         L.mfista_dft_profile.argtypes = [_dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp]
+        L.mfista_release_cache.restype = None
+        L.mfista_release_cache.argtypes = []
         L.mfista_nufft_movie.restype = C.c_int
         L.mfista_nufft_movie.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, C.c_int, C.c_int, C.c_int, _dp, C.c_double,
                                          C.c_double, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int, _dp,
@@ -169,6 +171,11 @@ def lib():
 def set_device(device):
     """CUDA device for this thread's subsequent calls."""
     _check(lib().mfista_set_device(int(device)))
+
+
+def release_cache():
+    """Free the solvers mfista_imaging_core_nufft keeps between calls."""
+    lib().mfista_release_cache()
 
 
 def set_fgp_iter(n):

@@ -6,6 +6,8 @@
 // itself runs on the GPU through mf::Solver.
 #include <time.h>
 
+#include <mutex>
+
 #include "solver.cuh"
 #include "looe.cuh"
 #include "cpp_nufft.cuh"
@@ -83,7 +85,94 @@ void run_single(MakeOp make_op, int N, int NX, int NY, int form, const float* bo
   out = o[0];
 }
 
+// Solvers of the NUFFT drop-in entry kept between calls.  A driver that
+// calls mfista_imaging_core_nufft repeatedly on one uv coverage (a lambda
+// sweep, a series of epochs) would otherwise rebuild the operator (point
+// binning, device buffers, FFT tables) and capture the solve graph on every
+// call.  An entry is keyed by everything that shapes the device data except
+// the visibilities: sizes, regulariser form, FGP iterations, device, and the
+// contents of u, v, vis_std and the box mask (compared exactly); a hit
+// uploads vis_r / vis_i and runs the captured graph.  At most
+// kDropinEntries are kept (least recently used out); a call that finds its
+// entry busy (another thread) builds a solver of its own.
+// MFISTA_DROPIN_CACHE=0 turns the cache off; mfista_release_cache() frees it.
+struct DropinNufft {
+  int M = 0, Nx = 0, Ny = 0, form = 0, fgp = 0, device = 0, box = 0;
+  std::vector<double> u, v, s;
+  std::vector<float> cbox;
+  std::unique_ptr<Solver> S;
+  NufftOp<double>* op = nullptr;
+  bool busy = false;
+  unsigned long long used = 0;
+};
+constexpr size_t kDropinEntries = 4;
+std::mutex g_dropin_mu;
+// never destroyed: at process exit the CUDA runtime may already be gone
+std::vector<std::unique_ptr<DropinNufft>>& g_dropin = *new std::vector<std::unique_ptr<DropinNufft>>();
+unsigned long long g_dropin_clock = 0;
+
+bool dropin_cache_on() {
+  const char* c = getenv("MFISTA_DROPIN_CACHE");
+  return !(c && c[0] == '0');
+}
+
+// the cached solver matching the call, marked busy, or null
+DropinNufft* dropin_find(const double* u, const double* v, const double* s, int M, int Nx, int Ny, int form,
+                         const float* box, int device) {
+  std::lock_guard<std::mutex> lk(g_dropin_mu);
+  const size_t nb = box ? (size_t)Nx * Ny : 0;
+  for (auto& e : g_dropin) {
+    if (e->busy || e->M != M || e->Nx != Nx || e->Ny != Ny || e->form != form || e->fgp != g_fgp_iter ||
+        e->device != device || e->box != (box ? 1 : 0))
+      continue;
+    if (memcmp(e->u.data(), u, sizeof(double) * M) || memcmp(e->v.data(), v, sizeof(double) * M) ||
+        memcmp(e->s.data(), s, sizeof(double) * M) || (nb && memcmp(e->cbox.data(), box, sizeof(float) * nb)))
+      continue;
+    e->busy = true;
+    e->used = ++g_dropin_clock;
+    return e.get();
+  }
+  return nullptr;
+}
+
+// hands a solver back (kept = false: it failed and is dropped)
+void dropin_return(DropinNufft* e, bool fresh, bool kept) {
+  std::lock_guard<std::mutex> lk(g_dropin_mu);
+  if (!fresh) {
+    if (kept) {
+      e->busy = false;
+    } else {
+      for (size_t i = 0; i < g_dropin.size(); ++i)
+        if (g_dropin[i].get() == e) {
+          g_dropin.erase(g_dropin.begin() + i);
+          break;
+        }
+    }
+    return;
+  }
+  std::unique_ptr<DropinNufft> own(e);
+  if (!kept) return;
+  own->busy = false;
+  own->used = ++g_dropin_clock;
+  while (g_dropin.size() >= kDropinEntries) {  // least recently used, not busy
+    size_t victim = g_dropin.size();
+    for (size_t i = 0; i < g_dropin.size(); ++i)
+      if (!g_dropin[i]->busy && (victim == g_dropin.size() || g_dropin[i]->used < g_dropin[victim]->used)) victim = i;
+    if (victim == g_dropin.size()) return;  // all busy: do not keep this one
+    g_dropin.erase(g_dropin.begin() + victim);
+  }
+  g_dropin.push_back(std::move(own));
+}
+
 }  // namespace
+
+extern "C" void mfista_release_cache(void) {
+  std::lock_guard<std::mutex> lk(g_dropin_mu);
+  for (size_t i = 0; i < g_dropin.size();) {
+    if (g_dropin[i]->busy) ++i;
+    else g_dropin.erase(g_dropin.begin() + i);
+  }
+}
 
 extern "C" int mfista_last_status(void) { return g_status; }
 extern "C" int mfista_set_device(int device) {
@@ -133,19 +222,63 @@ extern "C" void mfista_imaging_core_nufft(double* u_dx, double* v_dy, double* vi
     printf("stop if iter = %d, or Delta_cost < %e\n", maxiter, epsilon);
     if (skip) printf("nonneg_flag must be chosen properly.\n");
   }
+  DropinNufft* E = nullptr;
+  bool fresh = false;
   try {
     ProbParams p{lambda_l1, lambda_tv, lambda_tsv, cinit, epsilon, maxiter, nonneg_flag, box_flag, 0, 0.0};
     NufftInput in{u_dx, v_dy, vis_r, vis_i, vis_std, nullptr, 1, M, Nx, Ny};
     FinalOut o;
     double ct;
     std::vector<double> xo(skip ? xout : xinit, (skip ? xout : xinit) + (size_t)Nx * Ny);
-    run_single([&](Ctx& c) { return new NufftOp<double>(c, in); }, Nx * Ny, Nx, Ny, form,
-               box_flag == 1 ? cl_box : nullptr, p, xo.data(), skip, xo.data(), o, ct);
+    const float* box = box_flag == 1 ? cl_box : nullptr;
+    if (skip || !dropin_cache_on() || M < 1) {
+      run_single([&](Ctx& c) { return new NufftOp<double>(c, in); }, Nx * Ny, Nx, Ny, form, box, p, xo.data(), skip,
+                 xo.data(), o, ct);
+    } else {
+      int dev = 0;
+      MF_CK(cudaGetDevice(&dev));
+      E = dropin_find(u_dx, v_dy, vis_std, M, Nx, Ny, form, box, dev);
+      if (E) {  // same geometry: new visibilities into the kept operator
+        MF_CK(cudaMemcpy(E->op->d_vr.p, vis_r, sizeof(double) * M, cudaMemcpyHostToDevice));
+        MF_CK(cudaMemcpy(E->op->d_vi.p, vis_i, sizeof(double) * M, cudaMemcpyHostToDevice));
+      } else {
+        fresh = true;
+        E = new DropinNufft;
+        E->M = M;
+        E->Nx = Nx;
+        E->Ny = Ny;
+        E->form = form;
+        E->fgp = g_fgp_iter;
+        E->device = dev;
+        E->box = box ? 1 : 0;
+        E->u.assign(u_dx, u_dx + M);
+        E->v.assign(v_dy, v_dy + M);
+        E->s.assign(vis_std, vis_std + M);
+        if (box) E->cbox.assign(box, box + (size_t)Nx * Ny);
+        E->busy = true;
+        E->S.reset(new Solver);
+        E->S->precision = MFISTA_FP64;
+        E->S->init_common(1, Nx * Ny, Nx, Ny, form, g_fgp_iter, box);
+        E->op = new NufftOp<double>(E->S->ctx, in);
+        E->S->op.reset(E->op);
+        E->S->finish_setup();
+      }
+      const double t0 = now_s();
+      E->S->upload_problems({p}, xo.data());
+      E->S->enqueue_solve(false);
+      std::vector<FinalOut> ov;
+      E->S->fetch(xo.data(), ov);
+      ct = now_s() - t0;
+      o = ov[0];
+      dropin_return(E, fresh, o.status == 0);
+      E = nullptr;
+    }
     memcpy(xout, xo.data(), sizeof(double) * (size_t)Nx * Ny);
     fill_result(mfista_result, o, M / 2, (double)M, Nx, Ny, Nx * Ny, lambda_l1, lambda_tv, lambda_tsv, maxiter,
                 nonneg_flag, ct, skip, cinit);
     if (o.status) fail(o.status, "solver stopped early (status " + std::to_string(o.status) + ")", !quiet());
   } catch (const Error& e) {
+    if (E) dropin_return(E, fresh, false);
     fail(e.status, e.what(), true);
   }
 }
