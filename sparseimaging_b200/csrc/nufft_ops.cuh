@@ -985,8 +985,7 @@ struct ItcTile {
 // perm entries: point index (24 bits) | first-tap row - row0 (3 bits) << 24
 // | first-tap column - col0 (3 bits) << 27
 constexpr int kItcMaxPoints = 1 << 24;
-constexpr size_t kItcSmem =
-    sizeof(float) * ((size_t)kItcWin * kItcWin * 2 * kItcProb + 8 * 16 * 36 + 8 * kItcWin * 17);
+constexpr size_t kItcSmem = sizeof(float) * (size_t)kItcWin * kItcWin * 2 * kItcProb;  // the window
 
 // x = hi + lo: hi is x rounded to the TF32 grid (half-ulp up in magnitude,
 // by integer add and mask), lo = x - hi exactly; lo goes to the tensor core
@@ -1007,15 +1006,13 @@ __device__ __forceinline__ void mma_tf32_1688(float (&d)[4], const uint32_t (&a)
 // B-fragment loads of a warp (four consecutive c, eight n) over all banks
 __device__ __forceinline__ int itc_swz(int c) { return ((c >> 1) & 1) << 3; }
 
-static __global__ void __launch_bounds__(256, 2) k_nufft_interp_tc(
+static __global__ void __launch_bounds__(256, 3) k_nufft_interp_tc(
     NufftGeom<float> geo, const ItcTile* __restrict__ tiles, int ntc, const int* __restrict__ perm,
     const cplx<float>* __restrict__ gall, long gstride, int nx, int ny, double inv_mm,
     const ProbState* __restrict__ st, int gate, Partials part, int qchi, int nslots, cplx<float>* __restrict__ y2,
     int B, const double2* __restrict__ ax_base, double2* __restrict__ ax_out) {
   extern __shared__ __align__(16) float itc_smem[];
-  float* s_g = itc_smem;                                    // [32 * 32 cells][16]
-  float* s_wy = s_g + kItcWin * kItcWin * 2 * kItcProb;     // per warp [16 points][36]
-  float* s_wx = s_wy + 8 * 16 * 36;                         // per warp [32 rows][17] (16 points)
+  float* s_g = itc_smem;  // [32 * 32 cells][16]
   __shared__ int s_list[kItcProb];
   __shared__ int s_cnt[8];
   __shared__ double s_chi[8][kItcProb];
@@ -1045,43 +1042,22 @@ static __global__ void __launch_bounds__(256, 2) k_nufft_interp_tc(
   // operator fill): zero partials
   if ((int)threadIdx.x < nact && qchi >= 0)
     for (int sl = blockIdx.x + ntc; sl < nslots; sl += ntc) part.at(qchi, s_list[threadIdx.x])[sl] = 0.0;
-  // the block's separable factors (loads issued before the window's)
-  float fy[16], fx[16];
+  // lane (g, t) works on points g and g + 8 of the block: its A fragments
+  // are wy of those points at columns 8 kk + t (+ 4), loaded before the
+  // window's cells so that both sets of loads are in flight together
+  const int ka = __shfl_sync(0xffffffffu, kq, g), kb = __shfl_sync(0xffffffffu, kq, g + 8);
+  const int dra = __shfl_sync(0xffffffffu, drq, g), drb = __shfl_sync(0xffffffffu, drq, g + 8);
+  const int dca = __shfl_sync(0xffffffffu, dcq, g), dcb = __shfl_sync(0xffffffffu, dcq, g + 8);
+  const bool va = g < np, vb = g + 8 < np;
+  float fa[4][4];
 #pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    const int k = __shfl_sync(0xffffffffu, kq, i);
-    const int dr = __shfl_sync(0xffffffffu, drq, i), dc = __shfl_sync(0xffffffffu, dcq, i);
-    fy[i] = 0.f;
-    fx[i] = 0.f;
-    if (i < np) {
-      const int jy = lane - dc, jx = lane - dr;
-      if (jy >= 0 && jy < kTaps) fy[i] = geo.wy[(size_t)k * kTaps + jy];
-      if (jx >= 0 && jx < kTaps) fx[i] = geo.wx[(size_t)k * kTaps + jx];
-    }
-  }
-  // the epilogue's point data: lane (g, t) finishes points g and g + 8
-  const bool fin = on && grp == 0;
-  int kp[2];
-  double pw[2], pvr[2], pvi[2];
+  for (int kk = 0; kk < 4; ++kk)
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    kp[h] = __shfl_sync(0xffffffffu, kq, g + 8 * h);
-    pw[h] = pvr[h] = pvi[h] = 0.0;
-    if (fin && g + 8 * h < np) {
-      pw[h] = geo.weight[kp[h]];
-      pvr[h] = geo.vis_r[kp[h]];
-      pvi[h] = geo.vis_i[kp[h]];
-    }
-  }
-  // and the anchors' models the epilogue adds (corrected form)
-  double2 pab[2][2];
-#pragma unroll
-  for (int h = 0; h < 2; ++h)
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      pab[h][j] = make_double2(0.0, 0.0);
-      if (ax_base && fin && g + 8 * h < np && 4 * j + t < nact)
-        pab[h][j] = ax_base[(size_t)s_list[4 * j + t] * geo.y2_bstride + kp[h]];
+    for (int q = 0; q < 4; ++q) {
+      const bool second = q & 1;
+      const int jy = 8 * kk + t + 4 * (q >> 1) - (second ? dcb : dca);
+      fa[kk][q] = ((second ? vb : va) && jy >= 0 && jy < kTaps)
+                      ? geo.wy[(size_t)(second ? kb : ka) * kTaps + jy] : 0.f;
     }
   // the window: virtual cell -> stored cell, sign of the imaginary part
   for (int v = threadIdx.x; v < kItcWin * kItcWin; v += blockDim.x) {
@@ -1123,13 +1099,6 @@ static __global__ void __launch_bounds__(256, 2) k_nufft_interp_tc(
       *reinterpret_cast<float4*>(dst + ((2 * s) ^ sw)) = q;
     }
   }
-  float* wy_w = s_wy + warp * 16 * 36;
-  float* wx_w = s_wx + warp * kItcWin * 17;
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    wy_w[i * 36 + lane] = fy[i];
-    wx_w[lane * 17 + i] = fx[i];
-  }
   if (lane < kItcProb) s_chi[warp][lane] = 0.0;
   __syncthreads();
   const int nj = nact > 4 ? 2 : 1;  // n-tiles of 8 columns (4 problems) in use
@@ -1141,12 +1110,21 @@ static __global__ void __launch_bounds__(256, 2) k_nufft_interp_tc(
 #pragma unroll
     for (int kk = 0; kk < 4; ++kk)
 #pragma unroll
-      for (int q = 0; q < 4; ++q)
-        split_tf32(wy_w[(g + 8 * (q & 1)) * 36 + 8 * kk + t + 4 * (q >> 1)], ah[kk][q], al[kk][q]);
+      for (int q = 0; q < 4; ++q) split_tf32(fa[kk][q], ah[kk][q], al[kk][q]);
     const int nr = rhi - rlo + 1, per = (nr + ng - 1) / ng;
     const int r0 = rlo + grp * per, r1 = min(rhi + 1, r0 + per);
+    // row weights of points g and g + 8 (the next row's loaded a row ahead)
+    auto wxa = [&](int r) {
+      const int jx = r - dra;
+      return (va && jx >= 0 && jx < kTaps) ? geo.wx[(size_t)ka * kTaps + jx] : 0.f;
+    };
+    auto wxb = [&](int r) {
+      const int jx = r - drb;
+      return (vb && jx >= 0 && jx < kTaps) ? geo.wx[(size_t)kb * kTaps + jx] : 0.f;
+    };
+    float wa = r0 < r1 ? wxa(r0) : 0.f, wb = r0 < r1 ? wxb(r0) : 0.f;
     for (int r = r0; r < r1; ++r) {
-      const float wa = wx_w[r * 17 + g], wb = wx_w[r * 17 + g + 8];
+      const float wan = wxa(r + 1), wbn = wxb(r + 1);
       const float* grow = s_g + (size_t)r * kItcWin * (2 * kItcProb);
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
@@ -1170,6 +1148,8 @@ static __global__ void __launch_bounds__(256, 2) k_nufft_interp_tc(
           d[j][3] = fmaf(wb, ta[0][3] + ta[1][3], d[j][3]);
         }
       }
+      wa = wan;
+      wb = wbn;
     }
   }
   // row groups 1.. hand their partial sums to group 0 (through the window's
@@ -1181,7 +1161,7 @@ static __global__ void __launch_bounds__(256, 2) k_nufft_interp_tc(
     for (int q = 0; q < 8; ++q) s_part[(warp * 8 + q) * 32 + lane] = d[q >> 2][q & 3];
   }
   __syncthreads();
-  if (fin) {
+  if (on && grp == 0) {
     for (int gg = 1; gg < ng; ++gg) {
       const int w2 = blk + gg * nb;
 #pragma unroll
@@ -1191,8 +1171,9 @@ static __global__ void __launch_bounds__(256, 2) k_nufft_interp_tc(
     double chi[2] = {0.0, 0.0};
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      if (g + 8 * h < np) {
-        const int k = kp[h];
+      if (h ? vb : va) {
+        const int k = h ? kb : ka;
+        const double w = geo.weight[k], vr = geo.vis_r[k], vi = geo.vis_i[k];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
           const int slot = 4 * j + t;
@@ -1200,13 +1181,14 @@ static __global__ void __launch_bounds__(256, 2) k_nufft_interp_tc(
             const size_t e = (size_t)s_list[slot] * geo.y2_bstride + k;
             double fr = (double)d[j][2 * h] * inv_mm, fi = (double)d[j][2 * h + 1] * inv_mm;
             if (ax_base) {
-              fr += pab[h][j].x;
-              fi += pab[h][j].y;
+              const double2 ab = ax_base[e];
+              fr += ab.x;
+              fi += ab.y;
             }
             if (ax_out) ax_out[e] = make_double2(fr, fi);
-            const double rr = (pvr[h] - fr) * pw[h], ri = (pvi[h] - fi) * pw[h];
+            const double rr = (vr - fr) * w, ri = (vi - fi) * w;
             chi[j] += rr * rr + ri * ri;
-            if (y2) y2[e] = mk<float>((float)(rr * pw[h]), (float)(ri * pw[h]));
+            if (y2) y2[e] = mk<float>((float)(rr * w), (float)(ri * w));
           }
         }
       }
