@@ -34,12 +34,24 @@ constexpr int kPanel = 64;  // Cholesky / triangular-solve block width
 constexpr int kGT = 64;     // GEMM tile (rows and columns)
 constexpr int kGK = 16;     // GEMM k step
 
+// 8-byte asynchronous global -> shared copy; src_bytes 0 writes zeros
+__device__ __forceinline__ void cp_async8_zfill(void* smem_dst, const void* gmem_src, unsigned int src_bytes) {
+  const unsigned int d = (unsigned int)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(gmem_src), "r"(src_bytes) : "memory");
+}
+
 // C (m x n, ldc) = alpha op(A) op(B) + beta C, column-major; op(A)(i,p) is
 // A[p + i lda] when TA, else A[i + p lda]; op(B)(p,j) is B[j + p ldb] when
 // TB, else B[p + j ldb].  lower: tiles strictly above the diagonal are
 // skipped (the Cholesky reads the lower triangle only).  256 threads, a
 // 64 x 64 tile per CTA, 4 x 4 outputs per thread at rows tx + 16r and
-// columns ty + 16c.
+// columns ty + 16c.  The k steps are double-buffered: the copies of step
+// p + 1 (cp.async, element by element, zeros outside the matrices) are in
+// flight while step p is multiplied.  With beta != 0 the C tile is copied
+// into shared memory at the start, behind the k steps (the trailing
+// updates of the factorisation are rank-64: four k steps only).
+constexpr int kGLd = kGT + 1;  // shared row length (padded)
+constexpr size_t kGemmSmem = sizeof(double) * (2 * 2 * kGK * kGLd + kGT * kGT);
 template <bool TA, bool TB>
 __global__ void __launch_bounds__(256) k_looe_gemm(int m, int n, int k, double alpha, const double* __restrict__ A,
                                                    int lda, const double* __restrict__ B, int ldb, double beta,
@@ -48,15 +60,21 @@ __global__ void __launch_bounds__(256) k_looe_gemm(int m, int n, int k, double a
   if (info && *info) return;
   const int i0 = blockIdx.x * kGT, j0 = blockIdx.y * kGT;
   if (lower && i0 + kGT - 1 < j0) return;
-  __shared__ double As[kGK][kGT + 1];
-  __shared__ double Bs[kGK][kGT + 1];
+  extern __shared__ __align__(16) double gemm_smem[];
+  auto As = reinterpret_cast<double(*)[kGK][kGLd]>(gemm_smem);
+  auto Bs = reinterpret_cast<double(*)[kGK][kGLd]>(gemm_smem + 2 * kGK * kGLd);
+  double* Cs = gemm_smem + 4 * kGK * kGLd;  // [64 columns][64 rows]
   const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
-  double acc[4][4];
-#pragma unroll
-  for (int r = 0; r < 4; ++r)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
-  for (int p0 = 0; p0 < k; p0 += kGK) {
+  if (beta != 0.0) {
+    for (int e = t; e < kGT * kGT; e += 256) {
+      const int i = e & (kGT - 1), j = e >> 6;
+      const int gi = i0 + i, gj = j0 + j;
+      const bool v = gi < m && gj < n;
+      cp_async8_zfill(Cs + e, v ? C + (size_t)gi + (size_t)gj * ldc : C, v ? 8u : 0u);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  auto stage = [&](int buf, int p0) {
 #pragma unroll
     for (int q = 0; q < (kGT * kGK) / 256; ++q) {
       const int e = t + 256 * q;
@@ -69,9 +87,9 @@ __global__ void __launch_bounds__(256) k_looe_gemm(int m, int n, int k, double a
         p = e / kGT;
       }
       const int gi = i0 + i, gp = p0 + p;
-      double v = 0.0;
-      if (gi < m && gp < k) v = TA ? A[(size_t)gp + (size_t)gi * lda] : A[(size_t)gi + (size_t)gp * lda];
-      As[p][i] = v;
+      const bool va = gi < m && gp < k;
+      cp_async8_zfill(&As[buf][p][i], va ? (TA ? A + (size_t)gp + (size_t)gi * lda : A + (size_t)gi + (size_t)gp * lda) : A,
+                      va ? 8u : 0u);
       int j;
       if (TB) {
         j = e % kGT;
@@ -81,34 +99,53 @@ __global__ void __launch_bounds__(256) k_looe_gemm(int m, int n, int k, double a
         p = e % kGK;
       }
       const int gj = j0 + j, gq = p0 + p;
-      double w = 0.0;
-      if (gj < n && gq < k) w = TB ? B[(size_t)gj + (size_t)gq * ldb] : B[(size_t)gq + (size_t)gj * ldb];
-      Bs[p][j] = w;
+      const bool vb = gj < n && gq < k;
+      cp_async8_zfill(&Bs[buf][p][j], vb ? (TB ? B + (size_t)gj + (size_t)gq * ldb : B + (size_t)gq + (size_t)gj * ldb) : B,
+                      vb ? 8u : 0u);
     }
-    __syncthreads();
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  double acc[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+  const int nk = (k + kGK - 1) / kGK;
+  // (the C group, when there is one, is older than every step's group, so
+  // the waits below cover it too)
+  if (nk > 0) stage(0, 0);
+  for (int kt = 0; kt < nk; ++kt) {
+    if (kt + 1 < nk) stage((kt + 1) & 1, (kt + 1) * kGK);
+    else asm volatile("cp.async.commit_group;" ::: "memory");  // keeps one group per step
+    asm volatile("cp.async.wait_group 1;" ::: "memory");       // step kt has landed (this thread)
+    __syncthreads();                                           // and everyone's
+    const int bf = kt & 1;
 #pragma unroll
     for (int p = 0; p < kGK; ++p) {
       double a[4], b[4];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) a[r] = As[p][tx + 16 * r];
+      for (int r = 0; r < 4; ++r) a[r] = As[bf][p][tx + 16 * r];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) b[c] = Bs[p][ty + 16 * c];
+      for (int c = 0; c < 4; ++c) b[c] = Bs[bf][p][ty + 16 * c];
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
     }
+    __syncthreads();  // buffer bf is refilled by the copies issued next step
+  }
+  if (beta != 0.0) {
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     __syncthreads();
   }
 #pragma unroll
   for (int r = 0; r < 4; ++r)
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const int gi = i0 + tx + 16 * r, gj = j0 + ty + 16 * c;
-      if (gi < m && gj < n) {
-        double* cp = C + (size_t)gi + (size_t)gj * ldc;
-        *cp = alpha * acc[r][c] + (beta != 0.0 ? beta * *cp : 0.0);
-      }
+      const int li = tx + 16 * r, lj = ty + 16 * c;
+      const int gi = i0 + li, gj = j0 + lj;
+      if (gi < m && gj < n)
+        C[(size_t)gi + (size_t)gj * ldc] = alpha * acc[r][c] + (beta != 0.0 ? beta * Cs[lj * kGT + li] : 0.0);
     }
 }
 
@@ -281,6 +318,10 @@ struct Looe {
     d_part.alloc(sizeof(double) * 2 * (size_t)cdiv(M, 256));
     d_info.alloc(sizeof(int));
     d_out.alloc(sizeof(double) * 3);
+    set_smem(k_looe_gemm<false, false>, kGemmSmem);
+    set_smem(k_looe_gemm<false, true>, kGemmSmem);
+    set_smem(k_looe_gemm<true, false>, kGemmSmem);
+    set_smem(k_looe_gemm<true, true>, kGemmSmem);
   }
   ~Looe() {
     if (s) cudaStreamDestroy(s);
@@ -290,8 +331,8 @@ struct Looe {
   void gemm(int m, int n, int k, double alpha, const double* A, int lda, const double* B, int ldb, double beta,
             double* C, int ldc, int lower) {
     if (m <= 0 || n <= 0) return;
-    k_looe_gemm<TA, TB><<<dim3(cdiv(m, kGT), cdiv(n, kGT)), 256, 0, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C,
-                                                                          ldc, lower, d_info.as<int>());
+    k_looe_gemm<TA, TB><<<dim3(cdiv(m, kGT), cdiv(n, kGT)), 256, kGemmSmem, s>>>(m, n, k, alpha, A, lda, B, ldb, beta,
+                                                                                  C, ldc, lower, d_info.as<int>());
     MF_LAUNCH_CK();
   }
 
