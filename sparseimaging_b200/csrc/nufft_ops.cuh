@@ -952,6 +952,21 @@ __global__ void __launch_bounds__(256, 3) k_nufft_interp_group_fly(
   }
 }
 
+// asynchronous global -> shared copies (4, 8 or 16 bytes)
+__device__ __forceinline__ void cp_async(void* smem_dst, const void* gmem_src, int bytes) {
+  const unsigned int d = (unsigned int)__cvta_generic_to_shared(smem_dst);
+  if (bytes == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
+  else if (bytes == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem_src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // Interpolation on the tensor cores (FP32 form, shared geometry)
 //
@@ -1221,40 +1236,100 @@ static __global__ void __launch_bounds__(256, 3) k_nufft_interp_tc(
 // reference's NU_SIGN) and once mirrored (first tap (-mx - 12, -my - 12),
 // both weight vectors reversed, imaginary part kept), each with half the
 // residual.  A tile's list holds every virtual point with a tap on it
-// (built on the host), so a cell (row r, column c) with virtual coordinates
-// (mr, mc) (the reference's wrap: mr = r or r - 2Nx, mc = c or -Ny) is
+// (built on the host, padded to a multiple of 8 with empty entries), so a
+// cell (row r, column c) with virtual coordinates (mr, mc) (the reference's
+// wrap: mr = r or r - 2Nx, mc = c or -Ny) is
 //   sum_p wy_p[mc - my0_p] * (wx_p[mr - mx0_p] * y_p)      (taps outside: 0)
 // For one row that is a 16 (columns) x K (points) by K x 16 (problem
 // columns) product: warp w of the CTA takes tile row w and runs it as
 // mma.sync m16n8k8 TF32 with the operands split in two TF32 parts
-// (lo*hi + hi*lo + hi*hi, FP32 accumulation).  Points are staged 64 at a
-// time; the column weights (the A operand, shared by the eight rows) are
-// formed once per stage for all warps.  Long lists are cut into segments of
-// kStcSeg points run by separate CTAs, which leave their partial tiles in a
-// scratch buffer; the last of a tile's CTAs to finish (a ticket per tile and
-// problem chunk) adds the segments in segment order and writes the tile, so
-// the result does not depend on the order the CTAs ran in.
+// (lo*hi + hi*lo + hi*hi, FP32 accumulation).  Everything but the residual
+// depends on the geometry alone and is formed once, at plan creation
+// (k_stc_prep): the A operand (the column weights, split hi / lo) in
+// mma fragment order, 1 KB per 8 list entries, and the row weights wx at
+// each of the tile's 8 rows (read from L2 inside the product loop: staging
+// them in shared memory cost more in occupancy than it saved).  A launch
+// gathers the residuals of its segment's points into shared memory and runs
+// the products.  Long lists
+// are cut into segments of kStcSeg points run by separate CTAs, which leave
+// their partial tiles in a scratch buffer; the last of a tile's CTAs to
+// finish (a ticket per tile and problem chunk) adds the segments in segment
+// order and writes the tile, so the result does not depend on the order the
+// CTAs ran in.
 // ---------------------------------------------------------------------------
 constexpr int kStcRows = 8, kStcCols = 16;
 constexpr int kStcProb = 8;   // problems per CTA (16 real columns)
-constexpr int kStcStage = 64; // virtual points per stage
 constexpr int kStcSeg = 256;  // virtual points per CTA (longer lists are cut)
 struct StcItem {
   int tile;           // tile index (row-major over tile rows x tile columns)
-  int start, count;   // the segment's virtual points: list[start, start + count)
+  int start, count;   // the segment's list entries: [start, start + count), count a multiple of 8
   int seg, nseg;      // segment index and count of this tile
   int scratch;        // scratch slot of segment 0 of the tile (nseg > 1)
 };
 
+// geometry-only operands of the tensor-core spreading, one thread per
+// (group of 8 list entries, lane): the lane's A fragments (hi, lo) of the
+// group, and the row weights of entry (group, lane & 7) at the tile's rows
+// (lanes 0..7 only).  vlist: point | mirrored << 24, or -1 (padding);
+// etile: each entry's tile.
+static __global__ void k_stc_prep(const int* __restrict__ vlist, const int* __restrict__ etile, int nent,
+                                  const int* __restrict__ mxa, const int* __restrict__ mya,
+                                  const float* __restrict__ wxa, const float* __restrict__ wya, int nx, int ny,
+                                  int ntcol, float* __restrict__ afrag, float* __restrict__ bxg) {
+  const int gi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);  // group of 8 entries
+  const int lane = threadIdx.x & 31;
+  if (gi * 8 >= nent) return;
+  const int g = lane >> 2, t = lane & 3;
+  auto entry = [&](int e, int& k, int& x0, int& y0, int& fl) {
+    const int v = vlist[e];
+    if (v < 0) return false;
+    k = v & 0xffffff;
+    fl = (v >> 24) & 1;
+    x0 = fl ? -mxa[k] - kMSP : mxa[k] - (kMSP - 1);
+    y0 = fl ? -mya[k] - kMSP : mya[k] - (kMSP - 1);
+    return true;
+  };
+  float* out = afrag + ((size_t)gi * 32 + lane) * 8;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    // fragment element q: column g (+8 for q odd), point t (+4 for q >= 2)
+    const int cc = g + 8 * (q & 1), pe = gi * 8 + t + 4 * (q >> 1);
+    int k, x0, y0, fl;
+    float w = 0.f;
+    if (entry(pe, k, x0, y0, fl)) {
+      const int tcl = etile[pe] % ntcol;
+      const int col = tcl * kStcCols + cc;
+      const int mcol = col < ny ? col : -ny;
+      const int jy = mcol - y0;
+      if (col <= ny && jy >= 0 && jy < kTaps) w = wya[(size_t)k * kTaps + (fl ? kTaps - 1 - jy : jy)];
+    }
+    uint32_t hi, lo;
+    split_tf32(w, hi, lo);
+    out[q] = __uint_as_float(hi);
+    out[4 + q] = __uint_as_float(lo);
+  }
+  if (lane < 8) {
+    const int pe = gi * 8 + lane;
+    int k, x0, y0, fl;
+    const bool ok = entry(pe, k, x0, y0, fl);
+    const int tr = ok ? etile[pe] / ntcol : 0;
+    for (int r = 0; r < kStcRows; ++r) {
+      const int row = tr * kStcRows + r;
+      const int mrow = row < nx ? row : row - 2 * nx;
+      const int jx = mrow - x0;
+      float w = 0.f;
+      if (ok && row < 2 * nx && jx >= 0 && jx < kTaps) w = wxa[(size_t)k * kTaps + (fl ? kTaps - 1 - jx : jx)];
+      bxg[((size_t)gi * kStcRows + r) * 8 + lane] = w;
+    }
+  }
+}
+
 static __global__ void __launch_bounds__(256) k_nufft_spread_tc(
     NufftGeom<float> geo, const StcItem* __restrict__ items, const int* __restrict__ vlist,
-    const cplx<float>* __restrict__ y2, cplx<float>* __restrict__ gall, long gstride, int nx, int ny,
-    int ntcol, const ProbState* __restrict__ st, int gate, int B, float* __restrict__ scratch,
-    unsigned int* __restrict__ tickets) {
-  __shared__ float s_ah[kStcStage * 24], s_al[kStcStage * 24];  // [point][16 columns] (row stride 24)
-  __shared__ float s_y[kStcStage * 24];                          // [point][16 problem columns]
-  __shared__ float s_bx[8][kStcStage];                           // per warp (tile row): wx at that row
-  __shared__ int s_k[kStcStage], s_x0[kStcStage], s_y0[kStcStage], s_fl[kStcStage];
+    const float4* __restrict__ afrag, const float* __restrict__ bxg, const cplx<float>* __restrict__ y2,
+    cplx<float>* __restrict__ gall, long gstride, int nx, int ny, int ntcol, const ProbState* __restrict__ st,
+    int gate, int B, float* __restrict__ scratch, unsigned int* __restrict__ tickets) {
+  __shared__ float s_y[kStcSeg * 24];  // [entry][16 problem columns] (row stride 24: conflict-free B loads)
   __shared__ int s_list[kStcProb];
   __shared__ int s_cnt[8];
   __shared__ unsigned int s_ticket;
@@ -1265,87 +1340,42 @@ static __global__ void __launch_bounds__(256) k_nufft_spread_tc(
   const int g = lane >> 2, t = lane & 3;
   const int tr = it.tile / ntcol, tcl = it.tile - tr * ntcol;
   const int row = tr * kStcRows + warp;
-  const bool row_ok = row < 2 * nx;
-  const int mrow = row < nx ? row : row - 2 * nx;
   const int nj = nact > 4 ? 2 : 1;
+  // the chunk's half residuals of the segment's entries, imaginary sign of
+  // direct / mirrored taps (the only data that changes between launches)
+  for (int e = threadIdx.x; e < it.count * 2 * kStcProb; e += blockDim.x) {
+    const int q = e >> 4, n = e & 15, sl = n >> 1;
+    float v = 0.f;
+    const int code = vlist[it.start + q];
+    if (code >= 0 && sl < nact) {
+      const cplx<float> r = y2[(size_t)s_list[sl] * geo.y2_bstride + (code & 0xffffff)];
+      v = (n & 1) ? (((code >> 24) & 1) ? 0.5f * r.y : -0.5f * r.y) : 0.5f * r.x;
+    }
+    s_y[q * 24 + n] = v;
+  }
+  __syncthreads();
   float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
-  for (int base = it.start; base < it.start + it.count; base += kStcStage) {
-    const int np = min(kStcStage, it.start + it.count - base);
-    // the stage's virtual points
-    if (threadIdx.x < kStcStage) {
-      const int q = threadIdx.x;
-      int k = 0, x0 = 1 << 29, y0 = 1 << 29, fl = 0;  // padding: no tap anywhere
-      if (q < np) {
-        const int e = vlist[base + q];
-        k = e & 0xffffff;
-        fl = (e >> 24) & 1;
-        const int mx = geo.mx[k], my = geo.my[k];
-        x0 = fl ? -mx - kMSP : mx - (kMSP - 1);
-        y0 = fl ? -my - kMSP : my - (kMSP - 1);
-      }
-      s_k[q] = k;
-      s_x0[q] = x0;
-      s_y0[q] = y0;
-      s_fl[q] = fl;
-    }
-    __syncthreads();
-    // column weights (A operand) for the whole CTA, split hi / lo
-    for (int e = threadIdx.x; e < kStcStage * kStcCols; e += blockDim.x) {
-      const int q = e >> 4, cc = e & 15;
-      const int col = tcl * kStcCols + cc;
-      const int mcol = col < ny ? col : -ny;
-      const int jy = mcol - s_y0[q];
-      float w = 0.f;
-      if (col <= ny && jy >= 0 && jy < kTaps) w = geo.wy[(size_t)s_k[q] * kTaps + (s_fl[q] ? kTaps - 1 - jy : jy)];
-      uint32_t hi, lo;
-      split_tf32(w, hi, lo);
-      s_ah[q * 24 + cc] = __uint_as_float(hi);
-      s_al[q * 24 + cc] = __uint_as_float(lo);
-    }
-    // the chunk's half residuals, imaginary sign of direct / mirrored taps
-    for (int e = threadIdx.x; e < kStcStage * 2 * kStcProb; e += blockDim.x) {
-      const int q = e >> 4, n = e & 15, sl = n >> 1;
-      float v = 0.f;
-      if (q < np && sl < nact) {
-        const cplx<float> r = y2[(size_t)s_list[sl] * geo.y2_bstride + s_k[q]];
-        v = (n & 1) ? (s_fl[q] ? 0.5f * r.y : -0.5f * r.y) : 0.5f * r.x;
-      }
-      s_y[q * 24 + n] = v;
-    }
-    // this warp's row weights
-    for (int q = lane; q < kStcStage; q += 32) {
-      const int jx = mrow - s_x0[q];
-      float w = 0.f;
-      if (row_ok && jx >= 0 && jx < kTaps) w = geo.wx[(size_t)s_k[q] * kTaps + (s_fl[q] ? kTaps - 1 - jx : jx)];
-      s_bx[warp][q] = w;
-    }
-    __syncthreads();
-    const int nk = (np + 7) & ~7;
-    for (int kb = 0; kb < nk; kb += 8) {
-      const int p0 = (kb + t) * 24, p1 = (kb + t + 4) * 24;
-      uint32_t ah[4], al[4];
-      ah[0] = __float_as_uint(s_ah[p0 + g]);
-      ah[1] = __float_as_uint(s_ah[p0 + g + 8]);
-      ah[2] = __float_as_uint(s_ah[p1 + g]);
-      ah[3] = __float_as_uint(s_ah[p1 + g + 8]);
-      al[0] = __float_as_uint(s_al[p0 + g]);
-      al[1] = __float_as_uint(s_al[p0 + g + 8]);
-      al[2] = __float_as_uint(s_al[p1 + g]);
-      al[3] = __float_as_uint(s_al[p1 + g + 8]);
-      const float bx0 = s_bx[warp][kb + t], bx1 = s_bx[warp][kb + t + 4];
+  const int g0 = it.start >> 3;  // first group of 8 entries
+  for (int kb = 0; kb < it.count; kb += 8) {
+    const int gi = g0 + (kb >> 3);
+    const float4 h4 = __ldg(afrag + ((size_t)gi * 32 + lane) * 2);
+    const float4 l4 = __ldg(afrag + ((size_t)gi * 32 + lane) * 2 + 1);
+    const uint32_t ah[4] = {__float_as_uint(h4.x), __float_as_uint(h4.y), __float_as_uint(h4.z), __float_as_uint(h4.w)};
+    const uint32_t al[4] = {__float_as_uint(l4.x), __float_as_uint(l4.y), __float_as_uint(l4.z), __float_as_uint(l4.w)};
+    const float bx0 = __ldg(bxg + ((size_t)gi * kStcRows + warp) * 8 + t);
+    const float bx1 = __ldg(bxg + ((size_t)gi * kStcRows + warp) * 8 + t + 4);
+    const int p0 = (kb + t) * 24, p1 = (kb + t + 4) * 24;
 #pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        if (j < nj) {
-          uint32_t bh0, bl0, bh1, bl1;
-          split_tf32(bx0 * s_y[p0 + 8 * j + g], bh0, bl0);
-          split_tf32(bx1 * s_y[p1 + 8 * j + g], bh1, bl1);
-          mma_tf32_1688(d[j], al, bh0, bh1);
-          mma_tf32_1688(d[j], ah, bl0, bl1);
-          mma_tf32_1688(d[j], ah, bh0, bh1);
-        }
+    for (int j = 0; j < 2; ++j) {
+      if (j < nj) {
+        uint32_t bh0, bl0, bh1, bl1;
+        split_tf32(bx0 * s_y[p0 + 8 * j + g], bh0, bl0);
+        split_tf32(bx1 * s_y[p1 + 8 * j + g], bh1, bl1);
+        mma_tf32_1688(d[j], al, bh0, bh1);
+        mma_tf32_1688(d[j], ah, bl0, bl1);
+        mma_tf32_1688(d[j], ah, bh0, bh1);
       }
     }
-    __syncthreads();  // the next stage overwrites the staged points
   }
   // lane (g, t) holds columns g and g + 8 of its row, problems 4 j + t
   const size_t cstride = (size_t)gridDim.y * 2048;
@@ -1361,14 +1391,14 @@ static __global__ void __launch_bounds__(256) k_nufft_spread_tc(
     __threadfence();
 #pragma unroll
     for (int q = 0; q < 8; ++q) d[q >> 2][q & 3] = 0.f;
-    for (int s = 0; s < it.nseg; ++s) {
-      const float* part = scratch + (size_t)(it.scratch + s) * cstride + (size_t)blockIdx.y * 2048;
+    for (int sg = 0; sg < it.nseg; ++sg) {
+      const float* part = scratch + (size_t)(it.scratch + sg) * cstride + (size_t)blockIdx.y * 2048;
 #pragma unroll
       for (int q = 0; q < 8; ++q) d[q >> 2][q & 3] += __ldcg(part + (warp * 32 + lane) * 8 + q);
     }
     if (threadIdx.x == 0) tickets[(size_t)it.tile * gridDim.y + blockIdx.y] = 0u;  // for the next launch
   }
-  if (!row_ok) return;
+  if (row >= 2 * nx) return;
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int col = tcl * kStcCols + g + 8 * h;
@@ -1395,19 +1425,6 @@ static __global__ void __launch_bounds__(256) k_nufft_spread_tc(
 constexpr int kSpreadTile = 16;
 
 // asynchronous global -> shared copies (cp.async): 4, 8 or 16 bytes
-__device__ __forceinline__ void cp_async(void* smem_dst, const void* gmem_src, int bytes) {
-  const unsigned int d = (unsigned int)__cvta_generic_to_shared(smem_dst);
-  if (bytes == 16)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem_src) : "memory");
-  else if (bytes == 8)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem_src) : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 // shared-memory staging of one CTA of the spreading kernel: two buffers, so
 // the points of the next round are copied in while this round is summed

@@ -270,7 +270,7 @@ template <typename T> struct NufftOp : Op {
   // FP32, shared geometry: spreading on the tensor cores (k_nufft_spread_tc;
   // MFISTA_SPREAD_TC=0 selects the cluster kernel)
   bool spread_tc = false;
-  DevMem d_sitems, d_svlist, d_sscratch, d_stickets;
+  DevMem d_sitems, d_svlist, d_sscratch, d_stickets, d_safrag, d_sbx;
   int nsitems = 0, stc_cols = 0;
   // chi^2 partial slots every interpolation kernel of this operator writes
   // (at least its own CTA count; the extra CTAs write zeros), so that the
@@ -288,6 +288,11 @@ template <typename T> struct NufftOp : Op {
       const char* f2 = getenv("MFISTA_SPREAD_TC");
       spread_tc = !(f2 && f2[0] == '0');
     }
+    // with the tensor-core interpolation the points-per-warp knob only sets
+    // the FP64 anchor interpolation's and the model residual's partition:
+    // 8 points per warp (the autotuner's choice on the lambda grid) keeps
+    // the chi^2 slot count at the tile count
+    if (interp_tc) ippw = 8;
     nx = in.Nx;
     ny = in.Ny;
     B = ctx.B;
@@ -444,12 +449,17 @@ template <typename T> struct NufftOp : Op {
         for (int a : trs)
           for (int b : tcs) lists[(size_t)a * stc_cols + b].push_back(k | (fl << 24));
       }
-    std::vector<int> flat;
+    // every tile's list padded to a multiple of 8 (empty entries: -1), so that
+    // the groups of 8 entries of the prepared operands never straddle tiles
+    std::vector<int> flat, etile;
     std::vector<StcItem> items;
     int nscr = 0;
     for (int t = 0; t < nt; ++t) {
-      const int start = (int)flat.size(), cnt = (int)lists[t].size();
+      const int start = (int)flat.size();
+      const int cnt = ((int)lists[t].size() + 7) & ~7;
       flat.insert(flat.end(), lists[t].begin(), lists[t].end());
+      flat.resize((size_t)start + cnt, -1);
+      etile.resize(flat.size(), t);
       const int nseg = std::max(1, cdiv(cnt, kStcSeg));
       for (int sg = 0; sg < nseg; ++sg)
         items.push_back(StcItem{t, start + sg * kStcSeg, std::min(kStcSeg, cnt - sg * kStcSeg), sg, nseg, nscr});
@@ -458,8 +468,20 @@ template <typename T> struct NufftOp : Op {
     // launch order: longest segments first
     std::stable_sort(items.begin(), items.end(), [](const StcItem& a, const StcItem& b) { return a.count > b.count; });
     nsitems = (int)items.size();
+    const int nent = (int)flat.size(), ngrp = std::max(1, nent / 8);
     d_sitems.upload(items.data(), items.size());
     d_svlist.upload(flat.data(), std::max<size_t>(flat.size(), 1));
+    DevMem d_etile;
+    d_etile.upload(etile.data(), std::max<size_t>(etile.size(), 1));
+    d_safrag.alloc(sizeof(float) * (size_t)ngrp * 256);
+    d_sbx.alloc(sizeof(float) * (size_t)ngrp * kStcRows * 8);
+    if (nent > 0) {
+      k_stc_prep<<<cdiv(ngrp, 8), 256>>>(d_svlist.as<int>(), d_etile.as<int>(), nent, d_mx.as<int>(), d_my.as<int>(),
+                                          d_wx.as<float>(), d_wy.as<float>(), nx, ny, stc_cols, d_safrag.as<float>(),
+                                          d_sbx.as<float>());
+      MF_LAUNCH_CK();
+    }
+    MF_CK(cudaDeviceSynchronize());  // d_etile goes out of scope
     const int chunks = cdiv(B, kStcProb);
     d_sscratch.alloc(sizeof(float) * (size_t)std::max(nscr, 1) * chunks * 2048);
     d_stickets.alloc(sizeof(unsigned int) * (size_t)nt * chunks);
@@ -605,8 +627,9 @@ template <typename T> struct NufftOp : Op {
     if constexpr (sizeof(T) == 4) {
       if (spread_tc) {
         k_nufft_spread_tc<<<dim3(nsitems, cdiv(B, kStcProb)), 256, 0, s>>>(
-            geo, d_sitems.as<StcItem>(), d_svlist.as<int>(), d_y2.as<cplx<float>>(), g, gstride, nx, ny, stc_cols,
-            c.st, gate, B, d_sscratch.as<float>(), d_stickets.as<unsigned int>());
+            geo, d_sitems.as<StcItem>(), d_svlist.as<int>(), d_safrag.as<float4>(), d_sbx.as<float>(),
+            d_y2.as<cplx<float>>(), g, gstride, nx, ny, stc_cols, c.st, gate, B, d_sscratch.as<float>(),
+            d_stickets.as<unsigned int>());
         MF_LAUNCH_CK();
         return;
       }
