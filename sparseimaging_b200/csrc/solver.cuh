@@ -253,8 +253,9 @@ template <typename T> struct NufftOp : Op {
   FftHost<T> fh, fcol;
   NufftGeom<T> geo{};
   // default launch shapes: the autotuner's choice on the 128 x 128 lambda
-  // grid (FP32: 4 columns per CTA)
-  int rpc = 8, cpc = sizeof(T) == 4 ? 4 : 8, tile_r = 8, tile_c = 32, ntiles = 0;
+  // grid with the tensor-core interpolation and spreading (8 rows and 8
+  // columns per CTA)
+  int rpc = 8, cpc = 8, tile_r = 8, tile_c = 32, ntiles = 0;
   int ippw = SharedChunk<T>::kInterpPts;  // interpolation points per warp (shared geometry)
   int spread_cs = 8;                      // spreading cluster size (shared geometry)
   // FP32 grouped interpolation with taps formed on the fly (fewer registers;
