@@ -604,7 +604,7 @@ __global__ void k_init_state(ProbState* st, int B, int bad_nonneg_tsv) {
 
 
 // Conditional blocks of the device loop: sets the IF handles of the anchor
-// refresh block (has_ref) and of the gradient block for this step -- 1 when
+// refresh block (has_ref) and of the gradient block (has_grad) for this step -- 1 when
 // some problem needs it -- and counts the kernels that those blocks launch
 // (launched[0]).  With `lists` it also writes this step's problem lists of
 // the three loop gates (count, then indices in increasing order; see
@@ -612,7 +612,7 @@ __global__ void k_init_state(ProbState* st, int B, int bad_nonneg_tsv) {
 // problem's state.  One CTA of 256 threads; the blocks' kernels keep their
 // per-problem gates.
 __global__ void __launch_bounds__(256) k_select_blocks(const ProbState* __restrict__ st, int B, int has_ref,
-                                                       cudaGraphConditionalHandle h_ref,
+                                                       int has_grad, cudaGraphConditionalHandle h_ref,
                                                        cudaGraphConditionalHandle h_grad, int n_ref, int n_grad,
                                                        unsigned long long* __restrict__ launched,
                                                        int* __restrict__ lists) {
@@ -654,8 +654,8 @@ __global__ void __launch_bounds__(256) k_select_blocks(const ProbState* __restri
   r = __syncthreads_or(r);
   if (threadIdx.x == 0) {
     if (has_ref) cudaGraphSetConditional(h_ref, r ? 1u : 0u);
-    cudaGraphSetConditional(h_grad, g ? 1u : 0u);
-    launched[0] += (unsigned long long)((has_ref && r ? n_ref : 0) + (g ? n_grad : 0));
+    if (has_grad) cudaGraphSetConditional(h_grad, g ? 1u : 0u);
+    launched[0] += (unsigned long long)((has_ref && r ? n_ref : 0) + (has_grad && g ? n_grad : 0));
     if (lists)
       for (int q = 0; q < kGateLists; ++q) lists[(size_t)q * (B + 1)] = base[q];
   }

@@ -1247,6 +1247,12 @@ struct Solver {
   size_t fgp_smem_bytes = 0;
   long fgp_scratch_stride = 0;
   int per_step_launches = 0;
+  int loop_unroll = 4;  // steps per pass of the device loop (MFISTA_LOOP_UNROLL)
+  // the gradient block under an IF node (MFISTA_GRAD_IF=1), or launched
+  // every step with its kernels exiting at their per-problem gates (the
+  // default: a taken IF node cost about 15 us per step on B200, more than
+  // the empty launches of the steps that skip it; measured 1-3 % faster)
+  bool grad_if = false;
   int fixed_launches = 0;
   int ref_block_launches = 0, grad_block_launches = 0, rest_launches = 0;
   // movie mode (set_movie before finish_setup): the B problems are the
@@ -1356,6 +1362,8 @@ struct Solver {
     fixed_launches = 2 * (op->launches_forward() + 2) + 1 + (joint ? 2 : 0);
     const char* hl = getenv("MFISTA_HOST_LOOP");
     host_loop = hl && hl[0] == '1';
+    if (const char* lu = getenv("MFISTA_LOOP_UNROLL")) loop_unroll = std::max(1, std::min(8, atoi(lu)));
+    if (const char* gi = getenv("MFISTA_GRAD_IF")) grad_if = gi[0] != '0';
     build_graph();
     // set-up copies and memsets ran on the legacy stream, which the solver's
     // non-blocking streams do not wait for
@@ -1531,8 +1539,9 @@ struct Solver {
       cudaGraph_t g = nullptr;
       MF_CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, nullptr, nullptr));
       if (op->corrected()) MF_CK(cudaGraphConditionalHandleCreate(&h_ref, g, 0, 0));
-      MF_CK(cudaGraphConditionalHandleCreate(&h_grad, g, 0, 0));
-      k_select_blocks<<<1, 256, 0, s>>>(ctx.st, ctx.B, op->corrected() ? 1 : 0, h_ref, h_grad, ref_block_launches,
+      if (grad_if) MF_CK(cudaGraphConditionalHandleCreate(&h_grad, g, 0, 0));
+      k_select_blocks<<<1, 256, 0, s>>>(ctx.st, ctx.B, op->corrected() ? 1 : 0, grad_if ? 1 : 0, h_ref, h_grad,
+                                        ref_block_launches,
                                         grad_block_launches, d_steps.as<unsigned long long>() + 2,
                                         d_lists.as<int>());
       MF_LAUNCH_CK();
@@ -1546,7 +1555,7 @@ struct Solver {
       if (cond) end_if();
     }
     {
-      cudaStream_t bs = cond ? begin_if(s, h_grad) : s;
+      cudaStream_t bs = (cond && grad_if) ? begin_if(s, h_grad) : s;
       // gradient at z (only problems that start a new outer iteration)
       if (op->models_z()) op->forward_z(bs, kGateGrad, kQChiZ);
       else op->forward(bs, ctx.z, kGateGrad, kQChiZ, true);
@@ -1557,7 +1566,7 @@ struct Solver {
         k_movie_tgrad<<<ig, 256, 0, bs>>>(ctx.z, ctx.dfdx, dm, d_wt.as<double>(), lam_t, ctx.st, ctx.part);
         MF_LAUNCH_CK();
       }
-      if (cond) end_if();
+      if (cond && grad_if) end_if();
     }
     // trial point
     if (form == kFormTSV) {
@@ -1709,7 +1718,12 @@ struct Solver {
                                            cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
       return e;
     try {
-      enqueue_body(cap_stream, h, 1, true);
+      // the body holds loop_unroll steps: each pass of the WHILE node costs
+      // a device-side body launch (about 17 us measured between the last
+      // kernel of a step and the first of the next), paid once per
+      // loop_unroll steps; steps after every problem has stopped find all
+      // gates closed and change nothing
+      for (int u = 0; u < loop_unroll; ++u) enqueue_body(cap_stream, h, 1, true);
     } catch (...) {
       cudaGraph_t tmp;
       cudaStreamEndCapture(cap_block, &tmp);
@@ -1799,7 +1813,7 @@ struct Solver {
     unsigned long long h[3];
     MF_CK(cudaMemcpy(h, d_steps.p, sizeof(h), cudaMemcpyDeviceToHost));
     if (!cond_blocks) return (long long)h[0] * per_step_launches;
-    return (long long)h[0] * (rest_launches + 1) + (long long)h[2];
+    return (long long)h[0] * (rest_launches + 1 + (grad_if ? 0 : grad_block_launches)) + (long long)h[2];
   }
 
   void enqueue_solve(bool skip_loop) {
