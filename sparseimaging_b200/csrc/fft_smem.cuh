@@ -74,10 +74,23 @@ __device__ __forceinline__ void stockham_stage(const cplx<T>* __restrict__ src, 
                                                int sign) {
   const int nR = n / R;
   const int tstride = n / (Ns * R);
+  // powers of two (the usual grid sizes): the index arithmetic as shifts and
+  // masks instead of integer divisions (the same indices)
+  const bool pow2 = ((nR & (nR - 1)) == 0) && ((Ns & (Ns - 1)) == 0);
+  const int lnR = __ffs(nR) - 1, lNs = __ffs(Ns) - 1;
   for (int t = threadIdx.x; t < count * nR; t += blockDim.x) {
-    int tr = t / nR;
-    int j = t - tr * nR;
-    int k = j % Ns;
+    int tr, j, k, jq;
+    if (pow2) {
+      tr = t >> lnR;
+      j = t & (nR - 1);
+      k = j & (Ns - 1);
+      jq = j >> lNs;
+    } else {
+      tr = t / nR;
+      j = t - tr * nR;
+      k = j % Ns;
+      jq = j / Ns;
+    }
     const cplx<T>* s = src + (size_t)tr * ld;
     cplx<T>* d = dst + (size_t)tr * ld;
     cplx<T> v[R];
@@ -91,7 +104,7 @@ __device__ __forceinline__ void stockham_stage(const cplx<T>* __restrict__ src, 
     else if (R == 4) bfly4<T>(v, sign);
     else if (R == 3) bfly3<T>(v, sign);
     else if (R == 5) bfly5<T>(v, sign);
-    int base = (j / Ns) * Ns * R + k;
+    int base = jq * Ns * R + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) d[base + r * Ns] = v[r];
   }

@@ -129,8 +129,9 @@ __global__ void k_nufft_rows_fwd(const double* __restrict__ xall, long xstride, 
   cplx<T>* g = gall + (size_t)b * gstride;
   int i0 = blockIdx.x * rows_per_cta;
   int nrows = min(rows_per_cta, nx - i0);
+  const int lh = ((h & (h - 1)) == 0) ? __ffs(h) - 1 : -1;  // power-of-two rows: shifts
   for (int t = threadIdx.x; t < nrows * h; t += blockDim.x) {
-    int rr = t / h, m = t - rr * h;
+    int rr = lh >= 0 ? t >> lh : t / h, m = t - rr * h;
     int i = i0 + rr;
     int j0 = uncentre_index(2 * m, ny), j1 = uncentre_index(2 * m + 1, ny);
     T a = 0, c = 0;
@@ -180,8 +181,10 @@ __global__ void k_nufft_cols(cplx<T>* __restrict__ gall, long gstride, int nx, i
   cplx<T>* g = gall + (size_t)b * gstride;
   int c0 = blockIdx.x * cols_per_cta;
   int nc = min(cols_per_cta, ncol - c0);
+  // columns per CTA a power of two (every shape the tuner offers): shifts
+  const int lc = ((cols_per_cta & (cols_per_cta - 1)) == 0) ? __ffs(cols_per_cta) - 1 : -1;
   for (int t = threadIdx.x; t < n0 * cols_per_cta; t += blockDim.x) {
-    int r = t / cols_per_cta, cc = t - r * cols_per_cta;
+    int r = lc >= 0 ? t >> lc : t / cols_per_cta, cc = t - r * cols_per_cta;
     if (cc >= nc) continue;
     cplx<T> v = mk<T>(0, 0);
     if (!load_pruned || uncentre_index(r, nx) >= 0) v = g[(size_t)r * ncol + c0 + cc];
@@ -190,7 +193,7 @@ __global__ void k_nufft_cols(cplx<T>* __restrict__ gall, long gstride, int nx, i
   __syncthreads();
   cplx<T>* R = smem_fft<T>(A, Bf, f2x, ld, nc, sign);
   for (int t = threadIdx.x; t < n0 * cols_per_cta; t += blockDim.x) {
-    int r = t / cols_per_cta, cc = t - r * cols_per_cta;
+    int r = lc >= 0 ? t >> lc : t / cols_per_cta, cc = t - r * cols_per_cta;
     if (cc >= nc) continue;
     if (store_pruned && uncentre_index(r, nx) < 0) continue;
     g[(size_t)r * ncol + c0 + cc] = R[cc * ld + r];
@@ -404,8 +407,9 @@ __global__ void k_nufft_rows_inv(const cplx<T>* __restrict__ gall, long gstride,
   int i0 = blockIdx.x * rows_per_cta;
   int nrows = min(rows_per_cta, nx - i0);
   // Z[k] = (X_k + conj X_{h-k}) + i conj(W^k) (X_k - conj X_{h-k}); DC/Nyquist real parts only
+  const int lh = ((h & (h - 1)) == 0) ? __ffs(h) - 1 : -1;  // power-of-two rows: shifts
   for (int t = threadIdx.x; t < nrows * h; t += blockDim.x) {
-    int rr = t / h, k = t - rr * h;
+    int rr = lh >= 0 ? t >> lh : t / h, k = t - rr * h;
     const cplx<T>* grow = g + (size_t)centre_index(i0 + rr, nx) * (ny + 1);
     cplx<T> xk = grow[k];
     cplx<T> xc = grow[h - k];
@@ -425,7 +429,7 @@ __global__ void k_nufft_rows_inv(const cplx<T>* __restrict__ gall, long gstride,
   const double* z = fuse ? tf.z + (size_t)b * xstride : nullptr;
   double acc[1] = {0.0};
   for (int t = threadIdx.x; t < nrows * ny; t += blockDim.x) {
-    int rr = t / ny, j = t - rr * ny;
+    int rr = lh >= 0 ? t >> lh : t / ny, j = t - rr * ny;
     int i = i0 + rr;
     int c = centre_index(j, ny);
     cplx<T> zc = Z[rr * ld + (c >> 1)];
