@@ -148,8 +148,9 @@ __global__ void k_nufft_rows_fwd(const double* __restrict__ xall, long xstride, 
   __syncthreads();
   cplx<T>* Z = smem_fft<T>(A, Bf, fh, ld, nrows, -1);
   // X[k] = 1/2[(Z_k + conj Z_{h-k}) - i W^k (Z_k - conj Z_{h-k})], W = exp(-2 pi i / 2h)
-  for (int t = threadIdx.x; t < nrows * (h + 1); t += blockDim.x) {
-    int rr = t / (h + 1), k = t - rr * (h + 1);
+  // a warp per row, lanes along its h + 1 outputs (no division by h + 1)
+  for (int rr = (int)(threadIdx.x >> 5); rr < nrows; rr += (int)(blockDim.x >> 5))
+    for (int k = (int)(threadIdx.x & 31); k <= h; k += 32) {
     cplx<T> zk = Z[rr * ld + (k == h ? 0 : k)];
     cplx<T> zc = cconj<T>(Z[rr * ld + (k == 0 ? 0 : h - k)]);
     cplx<T> e = cadd<T>(zk, zc);
