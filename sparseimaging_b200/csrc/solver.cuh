@@ -455,15 +455,18 @@ template <typename T> struct NufftOp : Op {
     std::vector<int> flat, etile;
     std::vector<StcItem> items;
     int nscr = 0;
+    // list entries per CTA: kStcSeg, or fewer (a multiple of 8) from MFISTA_SPREAD_SEG
+    int seg = kStcSeg;
+    if (const char* e = getenv("MFISTA_SPREAD_SEG")) seg = std::max(8, std::min(kStcSeg, atoi(e) & ~7));
     for (int t = 0; t < nt; ++t) {
       const int start = (int)flat.size();
       const int cnt = ((int)lists[t].size() + 7) & ~7;
       flat.insert(flat.end(), lists[t].begin(), lists[t].end());
       flat.resize((size_t)start + cnt, -1);
       etile.resize(flat.size(), t);
-      const int nseg = std::max(1, cdiv(cnt, kStcSeg));
+      const int nseg = std::max(1, cdiv(cnt, seg));
       for (int sg = 0; sg < nseg; ++sg)
-        items.push_back(StcItem{t, start + sg * kStcSeg, std::min(kStcSeg, cnt - sg * kStcSeg), sg, nseg, nscr});
+        items.push_back(StcItem{t, start + sg * seg, std::min(seg, cnt - sg * seg), sg, nseg, nscr});
       if (nseg > 1) nscr += nseg;
     }
     // launch order: longest segments first
