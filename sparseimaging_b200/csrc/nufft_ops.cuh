@@ -1264,7 +1264,7 @@ static __global__ void __launch_bounds__(256, 3) k_nufft_interp_tc(
 // ---------------------------------------------------------------------------
 constexpr int kStcRows = 8, kStcCols = 16;
 constexpr int kStcProb = 8;   // problems per CTA (16 real columns)
-constexpr int kStcSeg = 256;  // virtual points per CTA (longer lists are cut)
+constexpr int kStcSeg = 256;  // list entries per CTA at most (longer lists are cut)
 struct StcItem {
   int tile;           // tile index (row-major over tile rows x tile columns)
   int start, count;   // the segment's list entries: [start, start + count), count a multiple of 8
