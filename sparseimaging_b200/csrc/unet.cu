@@ -2,7 +2,7 @@
 // BF16 weights, FP32 activations and accumulation) that maps the dirty
 // image and the dirty beam of a problem to an initial image (clamped >= 0).
 // It has no counterpart in the reference; MFISTA always runs from its output
-// to the reference's own stopping rule, so the solver stays the judge.
+// to the reference's own stopping rule, which alone decides when it stops.
 //
 // Everything runs on the GPU with the kernels of this file: 3x3 convolutions
 // (forward; backward-data as the forward kernel over flipped, transposed

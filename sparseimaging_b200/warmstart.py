@@ -4,7 +4,7 @@ A U-Net (csrc/unet.cu: 4 levels, 16-32-64-128 channels, BF16 weights, FP32
 accumulation, trained on the GPU by the library's own kernels) maps the
 dirty image A^H W^2 y and the dirty beam A^H W^2 1 of a problem to an
 initial image.  MFISTA then runs from that image with the reference's own
-stopping rule, so the solver stays the judge; per problem the start is used
+stopping rule, which alone decides when it stops; per problem the start is used
 only when its objective is below that of the zero image (zero init is the
 fallback, `choose_starts`).
 
