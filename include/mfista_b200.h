@@ -111,7 +111,9 @@ const char *mfista_last_error(void);
  * per device): a call with the same uv points, vis_std, sizes, regulariser
  * form, FGP iterations and box mask as a kept one reuses its device buffers
  * and captured solve graph and only uploads the new visibilities.  This
- * frees them (solvers in use by another thread stay).  Setting
+ * frees them (solvers in use by another thread stay); call it before a
+ * cudaDeviceReset (a kept solver found without its device memory is not
+ * reused, but its addresses are not freed either).  Setting
  * MFISTA_DROPIN_CACHE=0 in the environment disables the cache. */
 void mfista_release_cache(void);
 

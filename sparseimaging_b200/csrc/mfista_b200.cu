@@ -103,6 +103,7 @@ struct DropinNufft {
   std::unique_ptr<Solver> S;
   NufftOp<double>* op = nullptr;
   bool busy = false;
+  bool stale = false;  // its device memory is gone (a reset): never reused, evicted first
   unsigned long long used = 0;
 };
 constexpr size_t kDropinEntries = 4;
@@ -122,12 +123,20 @@ DropinNufft* dropin_find(const double* u, const double* v, const double* s, int 
   std::lock_guard<std::mutex> lk(g_dropin_mu);
   const size_t nb = box ? (size_t)Nx * Ny : 0;
   for (auto& e : g_dropin) {
-    if (e->busy || e->M != M || e->Nx != Nx || e->Ny != Ny || e->form != form || e->fgp != g_fgp_iter ||
+    if (e->busy || e->stale || e->M != M || e->Nx != Nx || e->Ny != Ny || e->form != form || e->fgp != g_fgp_iter ||
         e->device != device || e->box != (box ? 1 : 0))
       continue;
     if (memcmp(e->u.data(), u, sizeof(double) * M) || memcmp(e->v.data(), v, sizeof(double) * M) ||
         memcmp(e->s.data(), s, sizeof(double) * M) || (nb && memcmp(e->cbox.data(), box, sizeof(float) * nb)))
       continue;
+    // a kept solver whose buffers no longer exist (cudaDeviceReset since)
+    // is dropped, not reused
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, e->op->d_vr.p) != cudaSuccess || pa.type != cudaMemoryTypeDevice) {
+      cudaGetLastError();
+      e->stale = true;
+      continue;
+    }
     e->busy = true;
     e->used = ++g_dropin_clock;
     return e.get();
@@ -157,8 +166,11 @@ void dropin_return(DropinNufft* e, bool fresh, bool kept) {
   while (g_dropin.size() >= kDropinEntries) {  // least recently used, not busy
     size_t victim = g_dropin.size();
     for (size_t i = 0; i < g_dropin.size(); ++i)
-      if (!g_dropin[i]->busy && (victim == g_dropin.size() || g_dropin[i]->used < g_dropin[victim]->used)) victim = i;
+      if (!g_dropin[i]->busy && (victim == g_dropin.size() || g_dropin[i]->stale ||
+                                 (!g_dropin[victim]->stale && g_dropin[i]->used < g_dropin[victim]->used)))
+        victim = i;
     if (victim == g_dropin.size()) return;  // all busy: do not keep this one
+    if (g_dropin[victim]->stale) (void)g_dropin[victim].release();  // see mfista_release_cache
     g_dropin.erase(g_dropin.begin() + victim);
   }
   g_dropin.push_back(std::move(own));
@@ -169,8 +181,14 @@ void dropin_return(DropinNufft* e, bool fresh, bool kept) {
 extern "C" void mfista_release_cache(void) {
   std::lock_guard<std::mutex> lk(g_dropin_mu);
   for (size_t i = 0; i < g_dropin.size();) {
-    if (g_dropin[i]->busy) ++i;
-    else g_dropin.erase(g_dropin.begin() + i);
+    if (g_dropin[i]->busy) {
+      ++i;
+      continue;
+    }
+    // a stale solver (its context reset under it) is left alone rather than
+    // destroyed: its addresses may belong to new allocations by now
+    if (g_dropin[i]->stale) (void)g_dropin[i].release();
+    g_dropin.erase(g_dropin.begin() + i);
   }
 }
 
