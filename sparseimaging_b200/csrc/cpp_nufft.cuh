@@ -330,7 +330,7 @@ struct CppNufftOp : Op {
   void grid_forward(cudaStream_t s, const double* src, int gate) {
     k_nufft_rows_fwd<double><<<dim3(cdiv(nx, fft->rpc), B), 256, fft->smem_rows, s>>>(
         src, c.xstride, d_e4.as<double>(), fft->d_grid.as<cplx<double>>(), fft->gstride, nx, ny, fft->fh.dev,
-        fft->tw2h.as<cplx<double>>(), c.st, gate, fft->rpc, nullptr);
+        fft->tw2h.as<cplx<double>>(), c.st, gate, fft->rpc, nullptr, DynUnits{nullptr, 0});
     MF_LAUNCH_CK();
     fft->launch_cols_fwd(s, gate);
   }
@@ -354,12 +354,12 @@ struct CppNufftOp : Op {
                                                 gate);
     MF_LAUNCH_CK();
     k_nufft_cols<double><<<dim3(cdiv(ny + 1, fft->cpc), B), 256, fft->smem_cols, s>>>(
-        g, fft->gstride, nx, ny, fft->fcol.dev, +1, fft->cpc, 0, 1, c.st, gate);
+        g, fft->gstride, nx, ny, fft->fcol.dev, +1, fft->cpc, 0, 1, c.st, gate, DynUnits{nullptr, 0});
     MF_LAUNCH_CK();
     TsvFuse tf{z_tsv, c.prm, c.tsvNX, c.tsvNY};
     k_nufft_rows_inv<double><<<dim3(cdiv(nx, fft->rpc), B), 256, fft->smem_rows, s>>>(
         g, fft->gstride, dst, c.xstride, d_e4.as<double>(), nx, ny, 1.0, fft->fh.dev, fft->tw2h.as<cplx<double>>(),
-        tf, c.part, qtsv, c.st, gate, fft->rpc);
+        tf, c.part, qtsv, c.st, gate, fft->rpc, DynUnits{nullptr, 0});
     MF_LAUNCH_CK();
   }
 

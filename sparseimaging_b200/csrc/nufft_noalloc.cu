@@ -209,8 +209,9 @@ extern "C" int mfista_nufft_forward_noalloc(const double* u_dx, const double* v_
   k_nufft_prep_points<double><<<cdiv_i(M, T), T, 0, s>>>(u_dx, v_dy, mx, my, M, Nx, Ny, wx, wy);
   k_nufft_prep_e4<<<cdiv_i((long)Nx * Ny, T), T, 0, s>>>(e4, Nx, Ny);
   k_nufft_rows_fwd<double><<<dim3(Nx, 1), T, smem_rows, s>>>(x, (long)Nx * Ny, e4, grid, 0, Nx, Ny, fh, tw_2h, st,
-                                                              kGateAll, 1, nullptr);
-  k_nufft_cols<double><<<dim3(Ny + 1, 1), T, smem_cols, s>>>(grid, 0, Nx, Ny, fcol, -1, 1, 1, 0, st, kGateAll);
+                                                              kGateAll, 1, nullptr, DynUnits{nullptr, 0});
+  k_nufft_cols<double><<<dim3(Ny + 1, 1), T, smem_cols, s>>>(grid, 0, Nx, Ny, fcol, -1, 1, 1, 0, st, kGateAll,
+                                                              DynUnits{nullptr, 0});
   NufftGeom<double> geo;
   memset(&geo, 0, sizeof(geo));
   geo.mx = mx;

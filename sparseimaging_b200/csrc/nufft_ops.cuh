@@ -105,6 +105,44 @@ static __global__ void k_nufft_prep_e4(double* __restrict__ e4, int nx, int ny) 
   e4[t] = coeff * exp(taux * ti * ti + tauy * tj * tj);
 }
 
+// Work of a CTA of the FFT passes.  Normally CTA (x, y) transforms units
+// (rows or columns) [x u, x u + u) of problem y, if y passes the gate.
+// Inside the device loop, with few problems active (this step's list for
+// the launch's gate holds at most kDynFew), the launch's CTAs are instead
+// spread over the active problems only, each taking fewer units (halving
+// from `small` up to u until the grid holds the work), so that the few
+// transforms left run on many SMs.  A row's or column's transform is the
+// same arithmetic whatever the units per CTA, so the results do not change.
+constexpr int kDynFew = 4;
+struct DynUnits {
+  const int* list;  // this step's gate list (count, then problem indices), or null (fixed mapping)
+  int small;
+};
+struct FftWork {
+  int b, u0, units;
+};
+__device__ __forceinline__ bool fft_work(const DynUnits& d, const ProbState* __restrict__ st, int gate, int n,
+                                         int units, FftWork& w) {
+  if (d.list && d.list[0] <= kDynFew) {
+    const int nact = d.list[0];
+    const int cap = (int)(gridDim.x * gridDim.y);
+    int u = d.small;
+    while (u < units && nact * ((n + u - 1) / u) > cap) u = min(2 * u, units);
+    const int nseg = (n + u - 1) / u;
+    const int idx = (int)(blockIdx.y * gridDim.x + blockIdx.x);
+    if (idx >= nact * nseg) return false;
+    w.b = d.list[1 + idx / nseg];
+    w.u0 = (idx % nseg) * u;
+    w.units = u;
+    return true;
+  }
+  w.b = blockIdx.y;
+  if (!gate_ok(st[w.b], gate)) return false;
+  w.u0 = blockIdx.x * units;
+  w.units = units;
+  return w.u0 < n;
+}
+
 // ---------------------------------------------------------------------------
 // forward, pass 1: pad + E4 + real FFT of every image row (rows of the
 // 2Nx x 2Ny padded grid that hold image data), written to the half grid.
@@ -114,10 +152,11 @@ template <typename T>
 __global__ void k_nufft_rows_fwd(const double* __restrict__ xall, long xstride, const double* __restrict__ e4,
                                  cplx<T>* __restrict__ gall, long gstride, int nx, int ny, FftDev<T> fh,
                                  const cplx<T>* __restrict__ tw2h, const ProbState* __restrict__ st, int gate,
-                                 int rows_per_cta, const double* __restrict__ suball) {
+                                 int rows_per_cta, const double* __restrict__ suball, DynUnits dyn) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  int b = blockIdx.y;
-  if (!gate_ok(st[b], gate)) return;
+  FftWork w;
+  if (!fft_work(dyn, st, gate, nx, rows_per_cta, w)) return;
+  const int b = w.b;
   const int h = ny;
   const int ld = h + 1;
   cplx<T>* A = reinterpret_cast<cplx<T>*>(smem_raw);
@@ -127,8 +166,8 @@ __global__ void k_nufft_rows_fwd(const double* __restrict__ xall, long xstride, 
   // back in FP64 at the interpolation)
   const double* sub = suball ? suball + (size_t)b * xstride : nullptr;
   cplx<T>* g = gall + (size_t)b * gstride;
-  int i0 = blockIdx.x * rows_per_cta;
-  int nrows = min(rows_per_cta, nx - i0);
+  int i0 = w.u0;
+  int nrows = min(w.units, nx - i0);
   const int lh = ((h & (h - 1)) == 0) ? __ffs(h) - 1 : -1;  // power-of-two rows: shifts
   for (int t = threadIdx.x; t < nrows * h; t += blockDim.x) {
     int rr = lh >= 0 ? t >> lh : t / h, m = t - rr * h;
@@ -171,21 +210,23 @@ __global__ void k_nufft_rows_fwd(const double* __restrict__ xall, long xstride, 
 template <typename T>
 __global__ void k_nufft_cols(cplx<T>* __restrict__ gall, long gstride, int nx, int ny, FftDev<T> f2x, int sign,
                              int cols_per_cta, int load_pruned, int store_pruned,
-                             const ProbState* __restrict__ st, int gate) {
+                             const ProbState* __restrict__ st, int gate, DynUnits dyn) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  int b = blockIdx.y;
-  if (!gate_ok(st[b], gate)) return;
+  FftWork w;
+  if (!fft_work(dyn, st, gate, ny + 1, cols_per_cta, w)) return;
+  const int b = w.b;
   const int n0 = 2 * nx, ncol = ny + 1;
   const int ld = n0 + 1;
   cplx<T>* A = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* Bf = A + (size_t)cols_per_cta * ld;
   cplx<T>* g = gall + (size_t)b * gstride;
-  int c0 = blockIdx.x * cols_per_cta;
-  int nc = min(cols_per_cta, ncol - c0);
+  const int cpc = w.units;
+  int c0 = w.u0;
+  int nc = min(cpc, ncol - c0);
   // columns per CTA a power of two (every shape the tuner offers): shifts
-  const int lc = ((cols_per_cta & (cols_per_cta - 1)) == 0) ? __ffs(cols_per_cta) - 1 : -1;
-  for (int t = threadIdx.x; t < n0 * cols_per_cta; t += blockDim.x) {
-    int r = lc >= 0 ? t >> lc : t / cols_per_cta, cc = t - r * cols_per_cta;
+  const int lc = ((cpc & (cpc - 1)) == 0) ? __ffs(cpc) - 1 : -1;
+  for (int t = threadIdx.x; t < n0 * cpc; t += blockDim.x) {
+    int r = lc >= 0 ? t >> lc : t / cpc, cc = t - r * cpc;
     if (cc >= nc) continue;
     cplx<T> v = mk<T>(0, 0);
     if (!load_pruned || uncentre_index(r, nx) >= 0) v = g[(size_t)r * ncol + c0 + cc];
@@ -193,8 +234,8 @@ __global__ void k_nufft_cols(cplx<T>* __restrict__ gall, long gstride, int nx, i
   }
   __syncthreads();
   cplx<T>* R = smem_fft<T>(A, Bf, f2x, ld, nc, sign);
-  for (int t = threadIdx.x; t < n0 * cols_per_cta; t += blockDim.x) {
-    int r = lc >= 0 ? t >> lc : t / cols_per_cta, cc = t - r * cols_per_cta;
+  for (int t = threadIdx.x; t < n0 * cpc; t += blockDim.x) {
+    int r = lc >= 0 ? t >> lc : t / cpc, cc = t - r * cpc;
     if (cc >= nc) continue;
     if (store_pruned && uncentre_index(r, nx) < 0) continue;
     g[(size_t)r * ncol + c0 + cc] = R[cc * ld + r];
@@ -395,18 +436,21 @@ template <typename T>
 __global__ void k_nufft_rows_inv(const cplx<T>* __restrict__ gall, long gstride, double* __restrict__ dall,
                                  long xstride, const double* __restrict__ e4, int nx, int ny, double inv_mm,
                                  FftDev<T> fh, const cplx<T>* __restrict__ tw2h, TsvFuse tf, Partials part,
-                                 int qtsv, const ProbState* __restrict__ st, int gate, int rows_per_cta) {
+                                 int qtsv, const ProbState* __restrict__ st, int gate, int rows_per_cta,
+                                 DynUnits dyn) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double sh[32];
-  int b = blockIdx.y;
-  if (!gate_ok(st[b], gate)) return;
+  FftWork w;
+  if (!fft_work(dyn, st, gate, nx, rows_per_cta, w)) return;
+  const int b = w.b;
   const int h = ny, ld = h + 1;
   cplx<T>* A = reinterpret_cast<cplx<T>*>(smem_raw);
   cplx<T>* Bf = A + (size_t)rows_per_cta * ld;
   const cplx<T>* g = gall + (size_t)b * gstride;
   double* dfdx = dall + (size_t)b * xstride;
-  int i0 = blockIdx.x * rows_per_cta;
-  int nrows = min(rows_per_cta, nx - i0);
+  // (the spread mapping only without TSV partials: their slots are the grid's x)
+  int i0 = w.u0;
+  int nrows = min(w.units, nx - i0);
   // Z[k] = (X_k + conj X_{h-k}) + i conj(W^k) (X_k - conj X_{h-k}); DC/Nyquist real parts only
   const int lh = ((h & (h - 1)) == 0) ? __ffs(h) - 1 : -1;  // power-of-two rows: shifts
   for (int t = threadIdx.x; t < nrows * h; t += blockDim.x) {

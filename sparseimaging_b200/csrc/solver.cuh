@@ -283,6 +283,7 @@ template <typename T> struct NufftOp : Op {
 
   NufftOp(Ctx& ctx, const NufftInput& in, bool correct = false) : c(ctx) {
     if (const char* f = getenv("MFISTA_INTERP_FLY")) interp_fly = f[0] == '1';
+    if (const char* f = getenv("MFISTA_FFT_DYN")) fft_dyn = f[0] != '0';
     if (sizeof(T) == 4 && in.shared != 0 && in.M < kItcMaxPoints) {
       const char* f = getenv("MFISTA_INTERP_TC");
       interp_tc = !(f && f[0] == '0');
@@ -532,6 +533,20 @@ template <typename T> struct NufftOp : Op {
   static size_t spread_smem() { return sizeof(cplx<T>) * SharedChunk<T>::kSpread * 256; }
   int spread_chunks() const { return cdiv(B, SharedChunk<T>::kSpread); }
 
+  // FFT passes inside the device loop: with few problems active the CTAs
+  // spread over them with fewer rows / columns each (fft_work, from the
+  // step's gate list); the fixed mapping elsewhere, or with MFISTA_FFT_DYN=0.
+  // A batch of at most kDynFew problems gets the grid of the small shape.
+  bool fft_dyn = true;
+  DynUnits dyn(int gate, int units) const {
+    const int sl = gate_list_slot(gate);
+    if (!fft_dyn || !c.act_lists || sl < 0 || units <= 2) return DynUnits{nullptr, 0};
+    return DynUnits{c.act_lists + (size_t)sl * (B + 1), 2};
+  }
+  int fft_grid(const DynUnits& d, int n, int units) const {
+    return cdiv(n, (d.list && B <= kDynFew) ? d.small : units);
+  }
+
   // the geometry with this launch's gate lists (set inside the device loop)
   NufftGeom<T> geo_now() const {
     NufftGeom<T> g = geo;
@@ -567,9 +582,10 @@ template <typename T> struct NufftOp : Op {
   }
 
   void launch_rows_fwd(cudaStream_t s, const double* src, int gate, const double* sub) {
-    k_nufft_rows_fwd<T><<<dim3(cdiv(nx, rpc), B), 256, smem_rows, s>>>(src, c.xstride, geo.e4, d_grid.as<cplx<T>>(),
-                                                                       gstride, nx, ny, fh.dev, tw2h.as<cplx<T>>(),
-                                                                       c.st, gate, rpc, sub);
+    const DynUnits d = dyn(gate, rpc);
+    k_nufft_rows_fwd<T><<<dim3(fft_grid(d, nx, rpc), B), 256, smem_rows, s>>>(
+        src, c.xstride, geo.e4, d_grid.as<cplx<T>>(), gstride, nx, ny, fh.dev, tw2h.as<cplx<T>>(), c.st, gate, rpc,
+        sub, d);
     MF_LAUNCH_CK();
   }
 
@@ -621,8 +637,9 @@ template <typename T> struct NufftOp : Op {
   }
 
   void launch_cols_fwd(cudaStream_t s, int gate) {
-    k_nufft_cols<T><<<dim3(cdiv(ny + 1, cpc), B), 256, smem_cols, s>>>(d_grid.as<cplx<T>>(), gstride, nx, ny,
-                                                                       fcol.dev, -1, cpc, 1, 0, c.st, gate);
+    const DynUnits d = dyn(gate, cpc);
+    k_nufft_cols<T><<<dim3(fft_grid(d, ny + 1, cpc), B), 256, smem_cols, s>>>(
+        d_grid.as<cplx<T>>(), gstride, nx, ny, fcol.dev, -1, cpc, 1, 0, c.st, gate, d);
     MF_LAUNCH_CK();
   }
 
@@ -675,13 +692,15 @@ template <typename T> struct NufftOp : Op {
   void adjoint(cudaStream_t s, const double* z_tsv, int qtsv) override {
     cplx<T>* g = d_grid.as<cplx<T>>();
     launch_spread(s, g, kGateGrad);
-    k_nufft_cols<T><<<dim3(cdiv(ny + 1, cpc), B), 256, smem_cols, s>>>(g, gstride, nx, ny, fcol.dev, +1, cpc, 0, 1,
-                                                                       c.st, kGateGrad);
+    const DynUnits dc = dyn(kGateGrad, cpc);
+    k_nufft_cols<T><<<dim3(fft_grid(dc, ny + 1, cpc), B), 256, smem_cols, s>>>(g, gstride, nx, ny, fcol.dev, +1, cpc,
+                                                                               0, 1, c.st, kGateGrad, dc);
     MF_LAUNCH_CK();
     TsvFuse tf{z_tsv, c.prm, c.tsvNX, c.tsvNY};
-    k_nufft_rows_inv<T><<<dim3(cdiv(nx, rpc), B), 256, smem_rows, s>>>(
+    const DynUnits dr = qtsv < 0 ? dyn(kGateGrad, rpc) : DynUnits{nullptr, 0};
+    k_nufft_rows_inv<T><<<dim3(fft_grid(dr, nx, rpc), B), 256, smem_rows, s>>>(
         g, gstride, c.dfdx, c.xstride, geo.e4, nx, ny, inv_mm, fh.dev, tw2h.as<cplx<T>>(), tf, c.part, qtsv, c.st,
-        kGateGrad, rpc);
+        kGateGrad, rpc, dr);
     MF_LAUNCH_CK();
   }
 
@@ -749,19 +768,19 @@ template <typename T> struct NufftOp : Op {
         return B * N * 8 + N * 8 + B * half_rows * cs;
       case 3:
         k_nufft_cols<T><<<dim3(cdiv(ny + 1, cpc), B), 256, smem_cols, s>>>(g, gstride, nx, ny, fcol.dev, -1, cpc, 1, 0,
-                                                                           c.st, kGateTrial);
+                                                                           c.st, kGateTrial, DynUnits{nullptr, 0});
         MF_LAUNCH_CK();
         return B * (half_rows + G) * cs;
       case 4:
         k_nufft_cols<T><<<dim3(cdiv(ny + 1, cpc), B), 256, smem_cols, s>>>(g, gstride, nx, ny, fcol.dev, +1, cpc, 0, 1,
-                                                                           c.st, kGateGrad);
+                                                                           c.st, kGateGrad, DynUnits{nullptr, 0});
         MF_LAUNCH_CK();
         return B * (G + half_rows) * cs;
       case 5: {
         TsvFuse tf{c.z, c.prm, c.tsvNX, c.tsvNY};
         k_nufft_rows_inv<T><<<dim3(cdiv(nx, rpc), B), 256, smem_rows, s>>>(
             g, gstride, c.dfdx, c.xstride, geo.e4, nx, ny, inv_mm, fh.dev, tw2h.as<cplx<T>>(), tf, c.part, kQTsvZ,
-            c.st, kGateGrad, rpc);
+            c.st, kGateGrad, rpc, DynUnits{nullptr, 0});
         MF_LAUNCH_CK();
         return B * (half_rows * cs + 2 * N * 8) + N * 8;
       }
